@@ -1,0 +1,320 @@
+"""Benchmark of the B200 SOGRAND cubic decoder (one JSON line on rank 0).
+
+Workload (the 2.0 dB point of the "plain method at scale" configuration):
+100,000 codewords of the (16,8)^3 cubic product code per GPU, i.i.d. info
+bits, BPSK over AWGN at Eb/N0 = 2.0 dB (sigma of channel_sim.c), float64 LLR
+cubes generated on the device by the seeded generator; L = 3, Imax = 30,
+Tmax = UINT64_MAX.  A step decodes the whole batch.  The 3.3 GB of LLRs per
+GPU are larger than L2, so no flush is needed between steps.
+
+  value  codewords/s over all ranks, inputs resident in HBM, timed with CUDA
+         events on the decode stream, max over ranks
+  e2e    the same through the public C ABI with host buffers
+         (sg_decode_host: pinned host LLRs in, bits + statistics out)
+
+`--impl reference` times the reference's own CPU decoder
+(SOGRAND_C/cubic_decoder_final.c built from its sources into oracle/_ref,
+else the oracle restatement) on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "codewords/s & info Mb/s on 1 B200 at Eb/N0 2 dB, BER-matched vs plain & CPU"
+UNIT = "codewords/s"
+SEED = 20260101
+EBN0 = 2.0
+# bytes per codeword the decode must move: 4096 float64 in, 64 bytes of bits out
+ALG_BYTES_PER_CW = 4096 * 8 + 64
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names[1:], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: rank 0 times the reference decoder on all host cores."""
+    if rank != 0:
+        return
+    import sogrand_b200 as sg
+
+    cores = len(os.sched_getaffinity(0))
+    per_proc = args.ref_cw_per_core
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final_O2")
+    kind = "reference" if os.path.exists(ref_bin) else "port"
+    with tempfile.TemporaryDirectory() as td:
+        shards = []
+        for c in range(cores):
+            _, llr = sg.gen_llr(SEED, c * per_proc, per_proc, ebn0_db=EBN0)
+            f = os.path.join(td, f"llr{c}.bin")
+            llr.tofile(f)
+            shards.append(f)
+        times = []
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            if kind == "reference":
+                procs = [subprocess.Popen([ref_bin, f, f + ".dec"], stdout=subprocess.DEVNULL) for f in shards]
+                for p in procs:
+                    if p.wait() != 0:
+                        raise RuntimeError("reference decoder failed")
+            else:
+                procs = [subprocess.Popen([sys.executable, __file__, "--port-worker", f]) for f in shards]
+                for p in procs:
+                    if p.wait() != 0:
+                        raise RuntimeError("oracle worker failed")
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+    n = cores * per_proc
+    value = n / statistics.mean(times)
+    sample = (f"{n} codewords per step ({per_proc} per core) at {EBN0} dB, one unmodified "
+              f"cubic_decoder_final process per core" if kind == "reference" else
+              f"{n} codewords per step ({per_proc} per core), oracle restatement per core")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cubic (16,8)^3 SOGRAND decode, Eb/N0 {EBN0} dB, L=3 Imax=30 Tmax=inf",
+                   "sample": sample, "cores": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "info_mbps": value * 512 / 1e6,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def port_worker(path):
+    """Decode one LLR shard with the oracle restatement (CPU baseline leg)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_api import Oracle
+
+    llr = np.fromfile(path)
+    Oracle(os.path.join(ROOT, "oracle", "libsg_oracle.so")).decode(llr)
+
+
+def cpu_baseline(args):
+    """Bounded CPU sample on the host cores: same kind as the reference arm."""
+    import sogrand_b200 as sg
+
+    cores = len(os.sched_getaffinity(0))
+    per_proc = args.cpu_cw_per_core
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final_O2")
+    kind = "reference" if os.path.exists(ref_bin) else "port"
+    with tempfile.TemporaryDirectory() as td:
+        files = []
+        for c in range(cores):
+            _, llr = sg.gen_llr(SEED, c * per_proc, per_proc, ebn0_db=EBN0)
+            f = os.path.join(td, f"llr{c}.bin")
+            llr.tofile(f)
+            files.append(f)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            procs = [subprocess.Popen([ref_bin, f, f + ".dec"], stdout=subprocess.DEVNULL) for f in files]
+        else:
+            procs = [subprocess.Popen([sys.executable, __file__, "--port-worker", f]) for f in files]
+        ok = all(p.wait() == 0 for p in procs)
+        dt = time.perf_counter() - t0
+    n = cores * per_proc
+    return {"value": n / dt if ok else None, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{n} codewords at {EBN0} dB ({per_proc} per core, one process per core), {dt:.1f} s wall"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sogrand", choices=["sogrand", "reference"])
+    ap.add_argument("--n-cw", type=int, default=100000, help="codewords per GPU per step")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-cw-per-core", type=int, default=16)
+    ap.add_argument("--ref-cw-per-core", type=int, default=4)
+    ap.add_argument("--port-worker", default=None, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.port_worker:
+        port_worker(args.port_worker)
+        return
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import sogrand_b200 as sg
+    from sogrand_b200 import _lib
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    # every rank decodes its own codeword range of the same stream (no data-path collective)
+    n = args.n_cw
+    cw0 = rank * n
+    stream = torch.cuda.Stream(dev)
+    p = sg.params()
+    lib = _lib.load()
+    with torch.cuda.stream(stream):
+        info, llr = sg.gen_llr(SEED, cw0, n, ebn0_db=EBN0, device=dev, stream=stream.cuda_stream)
+        bits = torch.empty((n, 64), dtype=torch.uint8, device=dev)
+        stats = torch.empty((n, sg.STATS_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    stream.synchronize()
+
+    def decode_step():
+        _lib.check(lib.sg_decode_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), None, stats.data_ptr(),
+                                        stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        decode_step()
+    stream.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        decode_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dt = ev0.elapsed_time(ev1) / 1000.0
+    t_max = dt
+    if pg:
+        t = torch.tensor([dt], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * n * args.steps / t_max
+
+    # results of the timed run (one step's worth) for the sanity fields
+    st = sg.stats_from_device(stats)
+    ber = float((np.unpackbits(bits.cpu().numpy()) != np.unpackbits(info.cpu().numpy())).mean())
+    ng_per_cw = float(st["ng"].mean())
+
+    # end to end through the public C ABI with pinned host buffers
+    llr_h = torch.empty((n, 4096), dtype=torch.float64, pin_memory=True)
+    llr_h.copy_(llr)
+    bits_h = torch.empty((n, 64), dtype=torch.uint8, pin_memory=True)
+    stats_h = np.zeros(n, sg.STATS_DTYPE)
+    del llr
+    torch.cuda.empty_cache()
+    lib.sg_decode_host(llr_h.data_ptr(), n, C.byref(p), bits_h.data_ptr(), None, stats_h.ctypes.data)  # warm
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        _lib.check(lib.sg_decode_host(llr_h.data_ptr(), n, C.byref(p), bits_h.data_ptr(), None,
+                                      stats_h.ctypes.data))
+    e2e_dt = (time.perf_counter() - t0) / args.e2e_steps
+    if pg:
+        t = torch.tensor([e2e_dt], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_dt = float(t.item())
+    e2e = {"value": world * n / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": n * 4096 * 8,
+           "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
+           "api": "sg_decode_host (host buffers, copies inside the timed region)"}
+
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        hbm_peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+    achieved = n * ALG_BYTES_PER_CW / (dt / args.steps) / 1e9
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"cubic (16,8)^3 SOGRAND decode, {n} codewords per GPU per step, "
+                                   f"Eb/N0 {EBN0} dB, L=3 Imax=30 Tmax=inf",
+                       "codewords_per_gpu": n, "ebn0_db": EBN0, "parallelism": f"replicas{world}",
+                       "l2": "inputs (3.3 GB per GPU) larger than L2; no flush"},
+            "info_mbps": value * 512 / 1e6,
+            "ber": ber, "ng_per_codeword": ng_per_cw, "guesses_per_s": value * ng_per_cw,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None,
+                         "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},
+            "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

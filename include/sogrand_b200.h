@@ -1,0 +1,177 @@
+/* sogrand_b200.h -- C ABI of the B200 SOGRAND decoder for the (16,8)^3
+ * cubic product code.
+ *
+ * The reference has no library API: its decoder is a process,
+ *   cubic_decoder <input_llr_file> <output_file>
+ * (SOGRAND_C/cubic_decoder_final.c:62-314), with one internal per-line
+ * boundary, SOGRAND_bitSO (SOGRAND_C/cubic_decoder_final.c:521).  This
+ * library replaces both: sg_decode_file() is the process contract (same
+ * file formats, same statistics), sg_decode_host()/sg_decode_device() are
+ * the per-codeword loop of main() (:119-289) as a call, and sg_bitso_*()
+ * is SOGRAND_bitSO over a batch of lines.
+ *
+ * Conventions
+ *  - All entry points return sg_status; none calls exit().  The text of the
+ *    last error on the calling thread is available from sg_last_error().
+ *  - *_host entry points take host pointers and are synchronous.
+ *  - *_device entry points take device pointers on the current CUDA device,
+ *    enqueue work on `stream` (a cudaStream_t, NULL for the legacy default
+ *    stream) and return without synchronising.
+ *  - The caller owns every buffer.  The library keeps, per device, a
+ *    read-only table of error-pattern orders (15 MB) built on first use.
+ *  - LLR cube layout, as in the reference files: 4096 float64 per codeword,
+ *    index slice*256 + col*16 + row in the reference's (row, col, slice)
+ *    tensor terms (SOGRAND_C/cubic_decoder_final.c:434-437), i.e. the order
+ *    in which cubic_encoder writes bits (SOGRAND_C/cubic_encoder.c:89-97).
+ *  - Decoded bits: 64 bytes per codeword, the 512 info bits packed MSB
+ *    first in the order of hard_decision (SOGRAND_C/cubic_decoder_final.c:
+ *    393-415, packing :272-280).
+ */
+#ifndef SOGRAND_B200_H
+#define SOGRAND_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_N 16
+#define SG_K 8
+#define SG_CUBE 4096
+#define SG_INFO_BITS 512
+#define SG_INFO_BYTES 64
+#define SG_MAX_IMAX 50                  /* alpha[100] in the reference */
+#define SG_MAX_PHASES (3 * SG_MAX_IMAX)
+#define SG_MAX_L 8
+
+typedef enum {
+    SG_OK = 0,
+    SG_ERR_ARG = 1,       /* invalid argument or parameter */
+    SG_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    SG_ERR_NONFINITE = 3, /* an input LLR is NaN or infinite */
+    SG_ERR_IO = 4,        /* file could not be opened, read or written */
+    SG_ERR_NOMEM = 5,     /* host or device allocation failed */
+    SG_ERR_TIMEOUT = 6    /* a bounded device-side wait gave up */
+} sg_status;
+
+/* Decoder parameters (SOGRAND_C/cubic_decoder_final.c:94-102). */
+typedef struct {
+    int32_t L;        /* list size, 1..SG_MAX_L; reference 3 */
+    int32_t Imax;     /* iterations, 1..SG_MAX_IMAX; reference 30 */
+    uint64_t Tmax;    /* per-line abandonment cap, checked where the
+                         reference checks it (once per logistic weight);
+                         UINT64_MAX = none (reference) */
+    double thres;     /* list-confidence stop, reference 1 - 1e-5 */
+    /* extrinsic weight of each phase: phase p of iteration i (1-based,
+       p = 0 columns, 1 rows, 2 slices) uses alpha[3*(i-1) + p].  The
+       reference uses alpha[2i-2] for columns and alpha[2i-1] for rows and
+       slices of a constant 0.7 array (:101-102, :149, :188, :227). */
+    double alpha[SG_MAX_PHASES];
+} sg_params;
+
+/* Per-codeword statistics (the reference prints only their averages,
+ * :299-304; its int totals overflow above ~1,090 codewords at 2 dB). */
+typedef struct {
+    double iterations; /* 0.5 per phase run, as n_iter (:145, :184, :223) */
+    uint64_t ng;       /* guesses, summed over all line decodes (NG) */
+    uint64_t ng_p;     /* sum over phases of the largest line NG (NG_p) */
+    int32_t converged; /* 1: early termination fired; 0: Imax reached;
+                          -1: input not finite, codeword not decoded */
+    int32_t phases;    /* phases run */
+} sg_cw_stats;
+
+/* Totals of a file decode (the stdout block of :299-304). */
+typedef struct {
+    uint64_t blocks;
+    double total_iterations;
+    uint64_t total_ng;
+    uint64_t total_ng_p;
+    double seconds;    /* wall time of the whole call */
+} sg_run_summary;
+
+/* Reference parameters: L=3, Imax=30, Tmax=UINT64_MAX, thres=1-1e-5,
+ * alpha=0.7. */
+void sg_params_default(sg_params* p);
+
+/* Decode n_cw LLR cubes on the GPU (device pointers, asynchronous).
+ * d_llr must be 8-byte aligned (16-byte aligned uses bulk async copies).
+ * d_lapp (nullable): final L_APP cubes, 4096 float64 per codeword.
+ * d_stats (nullable): one sg_cw_stats per codeword.
+ * Replaces the per-codeword loop of main(), cubic_decoder_final.c:119-289. */
+sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
+                           uint8_t* d_bits, double* d_lapp, sg_cw_stats* d_stats,
+                           void* stream);
+
+/* Same with host buffers: copies in, decodes, copies out, synchronises.
+ * Returns SG_ERR_NONFINITE (after decoding the rest) if any codeword had a
+ * non-finite LLR; those codewords report converged = -1. */
+sg_status sg_decode_host(const double* llr, size_t n_cw, const sg_params* p,
+                         uint8_t* bits, double* lapp, sg_cw_stats* stats);
+
+/* SOGRAND_bitSO (cubic_decoder_final.c:521-585) on n_lines independent
+ * 16-LLR lines: d_llr [n_lines][16] -> d_lapp, d_le [n_lines][16],
+ * d_nguess [n_lines] (the N_guess output), d_ncw [n_lines] (nullable:
+ * codewords found, the reference's curL).  Device pointers, asynchronous. */
+sg_status sg_bitso_device(const double* d_llr, size_t n_lines, int32_t L, uint64_t Tmax,
+                          double thres, double* d_lapp, double* d_le, int32_t* d_nguess,
+                          int32_t* d_ncw, void* stream);
+sg_status sg_bitso_host(const double* llr, size_t n_lines, int32_t L, uint64_t Tmax,
+                        double thres, double* lapp, double* le, int32_t* nguess, int32_t* ncw);
+
+/* The process contract of cubic_decoder (cubic_decoder_final.c:62-314):
+ * reads whole cubes of float64 LLRs from in_path (a trailing partial cube is
+ * ignored, as the reference's fread loop does), writes packed bits to
+ * out_path (a final partial byte, never produced for 512-bit blocks, would
+ * be left-shifted), fills *summary (nullable).  Decodes in chunks of at most
+ * chunk_cw codewords (0 = automatic). */
+sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_params* p,
+                         size_t chunk_cw, sg_run_summary* summary);
+
+/* ---- synthetic source, encoder and channel (pipeline stages before the
+ * decoder: generate_bin.c, cubic_encoder.c, channel_sim.c).  The reference
+ * seeds with time(NULL) and rand(); these are seeded and counter-based, so
+ * codeword c of a stream is the same on host and device and independent of
+ * batching.  Noise is Gaussian by the Marsaglia polar method; LLR = 2y/s^2
+ * with s the noise deviation of channel_sim.c:34-39 (code dimension 3). */
+
+/* Noise deviation for Eb/N0 in dB, as channel_sim.c:34-39 computes it. */
+double sg_channel_sigma(double ebn0_db);
+
+/* Info bits of codewords [cw0, cw0+n_cw) of stream `seed`: 64 packed bytes
+ * each, the layout of generate_bin/comparator files. */
+sg_status sg_gen_info_host(uint64_t seed, uint64_t cw0, size_t n_cw, uint8_t* info);
+
+/* Systematic (16,8)^3 encoding of packed info blocks (cubic_encoder.c:
+ * 23-100): 64 bytes in, 4096 bytes of 0/1 code bits out per codeword. */
+sg_status sg_encode_host(const uint8_t* info, size_t n_cw, uint8_t* code_bits);
+
+/* Full synthetic channel output for codewords [cw0, cw0+n_cw): info bits
+ * (nullable) and float64 LLR cubes.  sigma > 0 fixes the noise deviation;
+ * sigma <= 0 draws each codeword's Eb/N0 uniformly from
+ * [ebn0_lo_db, ebn0_hi_db] with the decoder's own exp. */
+sg_status sg_gen_llr_host(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma,
+                          double ebn0_lo_db, double ebn0_hi_db, uint8_t* info, double* llr);
+sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma,
+                            double ebn0_lo_db, double ebn0_hi_db, uint8_t* d_info,
+                            double* d_llr, void* stream);
+
+/* ---- diagnostics */
+
+/* The order in which a line decode tests error patterns when its
+ * reliability shift is IC (the loops of sogrand_main_logic,
+ * cubic_decoder_final.c:642-744, with mountain_build :775-789).  Writes up to
+ * cap entries: bits 0..15 the pattern over reliability-sorted positions,
+ * bit 16 set on the first pattern of each logistic weight.  Entry 0 is the
+ * hard decision.  Returns the number of entries (65536 when cap allows). */
+size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap);
+
+const char* sg_status_string(sg_status s);
+const char* sg_last_error(void);    /* thread-local text of the last failure */
+const char* sg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOGRAND_B200_H */

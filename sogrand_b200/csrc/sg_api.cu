@@ -1,0 +1,852 @@
+/* sg_api.cu -- B200 SOGRAND cubic decoder: kernels and C ABI.
+ *
+ * Kernels
+ *   sg_decode_kernel   the whole iterative decode of a codeword per CTA
+ *                      (SOGRAND_C/cubic_decoder_final.c:119-289): the 32 KB
+ *                      channel cube arrives in shared memory by one bulk
+ *                      asynchronous copy (cp.async.bulk, completion on an
+ *                      mbarrier) and stays there with the 32 KB extrinsic
+ *                      cube for all iterations; 8 warps take the 256 lines
+ *                      of a phase from a shared counter and decode one line
+ *                      each (sg_line.cuh); after every phase one warp runs the
+ *                      early-termination test on the 256 hard-decision words.
+ *   sg_bitso_kernel    SOGRAND_bitSO on independent lines, one warp per line.
+ *   sg_gen_kernel      seeded source + encoder + AWGN channel (sg_gen.h).
+ *
+ * Built with -fmad=false: no floating-point contraction anywhere, as in the
+ * reference's plain gcc build; the exp/log routines use explicit FMAs.
+ */
+#include <cuda_runtime.h>
+
+#include <errno.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <chrono>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sogrand_b200.h"
+#include "sg_code.h"
+#include "sg_enum.h"
+#include "sg_gen.h"
+#include "sg_line.cuh"
+#include "sg_math.h"
+
+#define SG_THREADS 256
+#define SG_WARPS (SG_THREADS / 32)
+#define SG_SPIN_LIMIT (1ll << 22) /* bounded mbarrier polling */
+
+__device__ const double g_etab[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
+__device__ const double g_ltab[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
+
+/* ------------------------------------------------------------ device -- */
+
+struct SgDecodeArgs {
+    const double* llr;
+    uint8_t* bits;
+    double* lapp;
+    sg_cw_stats* stats;
+    const uint32_t* enum_tabs;
+    unsigned int* err;
+    unsigned long long n_cw;
+    int32_t L;
+    int32_t imax;
+    uint32_t tmax;
+    int32_t use_bulk;
+    double thres;
+    double alpha[SG_MAX_PHASES];
+};
+
+struct SgCwSmem {
+    double lch[SG_CUBE];
+    double le[SG_CUBE];
+    double etab[SG_EXP_TAB_LEN];
+    double ltab[SG_LOG_TAB_LEN];
+    SgWarpScratch ws[SG_WARPS];
+    uint16_t hdw[256];
+    unsigned long long mbar;
+    unsigned long long ng;
+    unsigned int ngmax;
+    int line_next;
+    int conv;
+    int bad;
+};
+
+/* Cube index of bit `i` of line `l` in phase `axis` (lines of the reference's
+ * column phase run along the stride-1 index, rows along stride 16, slices
+ * along stride 256; cubic_decoder_final.c:157-247). */
+__device__ __forceinline__ int sg_pos(int axis, int l, int i)
+{
+    const int a = l >> 4, b = l & 15;
+    if (axis == 0)
+        return a * 256 + b * 16 + i;
+    if (axis == 1)
+        return a * 256 + i * 16 + b;
+    return i * 256 + a * 16 + b;
+}
+
+/* Early termination (cubic_decoder_final.c:317-391) on the 256 line words
+ * of the phase just run: the hard decisions form a product codeword iff
+ * every word is a component codeword and the words satisfy the component
+ * parity equations along both other axes (bitwise).  Warp-wide. */
+__device__ __forceinline__ bool sg_is_codeword(const uint16_t* hdw, int lane)
+{
+    bool bad = false;
+    for (int q = lane; q < 256; q += 32) {
+        const uint32_t x = hdw[q];
+        bad |= ((x >> 8) & 0xffu) != c_ptab[x & 0xffu];
+    }
+    for (int q = lane; q < 128; q += 32) {
+        const int a = q >> 3, j = q & 7;
+        uint32_t acc = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++)
+            if ((c_prow[b] >> j) & 1u)
+                acc ^= hdw[a * 16 + b];
+        bad |= acc != hdw[a * 16 + 8 + j];
+    }
+    for (int q = lane; q < 128; q += 32) {
+        const int b = q >> 3, j = q & 7;
+        uint32_t acc = 0;
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+            if ((c_prow[a] >> j) & 1u)
+                acc ^= hdw[a * 16 + b];
+        bad |= acc != hdw[(8 + j) * 16 + b];
+    }
+    return !__any_sync(SG_FULL, bad);
+}
+
+__device__ __forceinline__ uint32_t sg_smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+extern __shared__ __align__(128) unsigned char sg_smem_raw[];
+
+__global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
+{
+    SgCwSmem& S = *reinterpret_cast<SgCwSmem*>(sg_smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < SG_EXP_TAB_LEN; i += SG_THREADS)
+        S.etab[i] = g_etab[i];
+    for (int i = tid; i < SG_LOG_TAB_LEN; i += SG_THREADS)
+        S.ltab[i] = g_ltab[i];
+    const uint32_t mbar = sg_smem_u32(&S.mbar);
+    if (tid == 0 && args.use_bulk) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase_bit = 0;
+    SgLineParams lp;
+    lp.L = args.L;
+    lp.tmax = args.tmax;
+    lp.thres = args.thres;
+
+    for (unsigned long long cw = blockIdx.x; cw < args.n_cw; cw += gridDim.x) {
+        const double* g = args.llr + cw * SG_CUBE;
+        if (args.use_bulk) {
+            if (tid == 0) {
+                /* order earlier generic-proxy reads of lch before the async write */
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+                             "r"((uint32_t)(SG_CUBE * 8))
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        sg_smem_u32(S.lch)),
+                    "l"(g), "r"((uint32_t)(SG_CUBE * 8)), "r"(mbar)
+                    : "memory");
+            }
+        } else {
+            for (int i = tid; i < SG_CUBE; i += SG_THREADS)
+                S.lch[i] = g[i];
+        }
+        for (int i = tid; i < SG_CUBE; i += SG_THREADS)
+            S.le[i] = 0.0;
+        if (tid == 0) {
+            S.ng = 0;
+            S.conv = 0;
+            S.bad = 0;
+        }
+        if (args.use_bulk && tid == 0) {
+            uint32_t ok = 0;
+            for (long long it = 0; it < SG_SPIN_LIMIT && !ok; it++) {
+                asm volatile(
+                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                    : "=r"(ok)
+                    : "r"(mbar), "r"(phase_bit)
+                    : "memory");
+            }
+            if (!ok) {
+                atomicOr(args.err, 1u);
+                S.bad = 2;
+            }
+        }
+        phase_bit ^= 1u;
+        __syncthreads();
+        if (S.bad == 2) /* the bulk copy never completed: skip this codeword */
+            break;
+        bool nonfinite = false;
+        for (int i = tid; i < SG_CUBE; i += SG_THREADS)
+            nonfinite |= !isfinite(S.lch[i]);
+        if (__syncthreads_or(nonfinite)) {
+            if (tid < SG_INFO_BYTES)
+                args.bits[cw * SG_INFO_BYTES + tid] = 0;
+            if (tid == 0 && args.stats) {
+                sg_cw_stats st;
+                st.iterations = 0;
+                st.ng = 0;
+                st.ng_p = 0;
+                st.converged = -1;
+                st.phases = 0;
+                args.stats[cw] = st;
+            }
+            __syncthreads();
+            continue;
+        }
+
+        int phases = 0;
+        unsigned long long ng_p = 0;
+        int axis_last = 0;
+        bool conv = false;
+        for (int iter = 1; iter <= args.imax && !conv; iter++) {
+            for (int axis = 0; axis < 3 && !conv; axis++) {
+                const double alpha = args.alpha[3 * (iter - 1) + axis];
+                if (tid == 0) {
+                    S.line_next = 0;
+                    S.ngmax = 0;
+                }
+                __syncthreads();
+                for (;;) {
+                    int l = 0;
+                    if (lane == 0)
+                        l = atomicAdd(&S.line_next, 1);
+                    l = __shfl_sync(SG_FULL, l, 0);
+                    if (l >= 256)
+                        break;
+                    const int pos = sg_pos(axis, l, lane & 15);
+                    double v = 1.0;
+                    if (lane < 16)
+                        v = __dadd_rn(S.lch[pos], __dmul_rn(alpha, S.le[pos])); /* L_ch + (alpha*L_E) */
+                    const SgLineResult r =
+                        sg_decode_line(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+                    if (lane < 16) {
+                        S.le[pos] = r.le;
+                        if (args.lapp)
+                            args.lapp[cw * SG_CUBE + pos] = r.lapp;
+                    }
+                    if (lane == 0) {
+                        S.hdw[l] = (uint16_t)r.hdword;
+                        atomicAdd(&S.ng, (unsigned long long)r.T);
+                        atomicMax(&S.ngmax, r.T);
+                    }
+                }
+                __syncthreads();
+                phases++;
+                axis_last = axis;
+                ng_p += S.ngmax;
+                if (warp == 0) {
+                    const bool c = sg_is_codeword(S.hdw, lane);
+                    if (lane == 0)
+                        S.conv = c;
+                }
+                __syncthreads();
+                conv = S.conv != 0;
+            }
+        }
+
+        /* hard_decision (:393-415): info bit b = s*64 + r*8 + c is the sign of
+         * L_APP at cube index s*256 + r*16 + c; packed MSB first (:272-280) */
+        if (tid < SG_INFO_BYTES) {
+            uint32_t byte = 0;
+            for (int q = 0; q < 8; q++) {
+                const int b = tid * 8 + q;
+                const int p = (b >> 6) * 256 + ((b >> 3) & 7) * 16 + (b & 7);
+                int l, bit;
+                if (axis_last == 0) {
+                    l = (p >> 8) * 16 + ((p >> 4) & 15);
+                    bit = p & 15;
+                } else if (axis_last == 1) {
+                    l = (p >> 8) * 16 + (p & 15);
+                    bit = (p >> 4) & 15;
+                } else {
+                    l = ((p >> 4) & 15) * 16 + (p & 15);
+                    bit = p >> 8;
+                }
+                byte = (byte << 1) | ((S.hdw[l] >> bit) & 1u);
+            }
+            args.bits[cw * SG_INFO_BYTES + tid] = (uint8_t)byte;
+        }
+        if (tid == 0 && args.stats) {
+            sg_cw_stats st;
+            st.iterations = 0.5 * phases;
+            st.ng = S.ng;
+            st.ng_p = ng_p;
+            st.converged = conv ? 1 : 0;
+            st.phases = phases;
+            args.stats[cw] = st;
+        }
+        __syncthreads();
+    }
+}
+
+struct SgLineSmem {
+    double etab[SG_EXP_TAB_LEN];
+    double ltab[SG_LOG_TAB_LEN];
+    SgWarpScratch ws[SG_WARPS];
+};
+
+__global__ void __launch_bounds__(SG_THREADS) sg_bitso_kernel(const double* __restrict__ llr,
+                                                               unsigned long long n_lines,
+                                                               SgLineParams lp, double* lapp, double* le,
+                                                               int32_t* nguess, int32_t* ncw,
+                                                               const uint32_t* enum_tabs)
+{
+    __shared__ SgLineSmem S;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < SG_EXP_TAB_LEN; i += SG_THREADS)
+        S.etab[i] = g_etab[i];
+    for (int i = tid; i < SG_LOG_TAB_LEN; i += SG_THREADS)
+        S.ltab[i] = g_ltab[i];
+    __syncthreads();
+    for (unsigned long long l = (unsigned long long)blockIdx.x * SG_WARPS + warp; l < n_lines;
+         l += (unsigned long long)gridDim.x * SG_WARPS) {
+        const double v = lane < 16 ? llr[l * 16 + lane] : 1.0;
+        if (__any_sync(SG_FULL, !isfinite(v))) { /* not decoded: NaN out, N_guess -1 */
+            if (lane < 16) {
+                lapp[l * 16 + lane] = __longlong_as_double(0x7ff8000000000000ll);
+                le[l * 16 + lane] = __longlong_as_double(0x7ff8000000000000ll);
+            }
+            if (lane == 0) {
+                nguess[l] = -1;
+                if (ncw)
+                    ncw[l] = 0;
+            }
+            continue;
+        }
+        const SgLineResult r = sg_decode_line(v, lp, enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+        if (lane < 16) {
+            lapp[l * 16 + lane] = r.lapp;
+            le[l * 16 + lane] = r.le;
+        }
+        if (lane == 0) {
+            nguess[l] = (int32_t)r.T;
+            if (ncw)
+                ncw[l] = r.ncw;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint64_t cw0,
+                                                             unsigned long long n_cw, double sigma,
+                                                             double lo, double hi, uint8_t* info,
+                                                             double* llr)
+{
+    __shared__ double etab[SG_EXP_TAB_LEN];
+    __shared__ double ltab[SG_LOG_TAB_LEN];
+    __shared__ uint16_t W[256];
+    __shared__ uint8_t ib[SG_INFO_BYTES];
+    __shared__ uint8_t prow[8];
+    __shared__ uint8_t ptab[256];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < SG_EXP_TAB_LEN; i += SG_THREADS)
+        etab[i] = g_etab[i];
+    for (int i = tid; i < SG_LOG_TAB_LEN; i += SG_THREADS)
+        ltab[i] = g_ltab[i];
+    if (tid < 8)
+        prow[tid] = c_prow[tid];
+    ptab[tid] = c_ptab[tid];
+    __syncthreads();
+    for (unsigned long long c = blockIdx.x; c < n_cw; c += gridDim.x) {
+        const uint64_t gc = cw0 + c;
+        if (tid < 8) {
+            const uint64_t r = sg_rand(seed, 0, gc * 8 + tid);
+            for (int q = 0; q < 8; q++)
+                ib[tid * 8 + q] = (uint8_t)(r >> (8 * q));
+        }
+        __syncthreads();
+        if (tid == 0)
+            sg_encode_words(ib, prow, ptab, W);
+        if (info && tid < SG_INFO_BYTES)
+            info[c * SG_INFO_BYTES + tid] = ib[tid];
+        __syncthreads();
+        const double s = sigma > 0.0 ? sigma : sg_sigma_draw(seed, gc, lo, hi, etab);
+        for (int p = tid; p < SG_CUBE; p += SG_THREADS) {
+            const int bit = (W[p >> 4] >> (p & 15)) & 1;
+            llr[c * SG_CUBE + p] = sg_llr_of(bit, s, sg_normal(seed, gc, (uint32_t)p, ltab));
+        }
+        __syncthreads();
+    }
+}
+
+/* -------------------------------------------------------------- host -- */
+
+namespace {
+
+thread_local std::string t_err;
+
+sg_status fail(sg_status s, const std::string& msg)
+{
+    t_err = msg;
+    return s;
+}
+
+sg_status cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(SG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SG_CUDA(call)                         \
+    do {                                      \
+        cudaError_t e_ = (call);              \
+        if (e_ != cudaSuccess)                \
+            return cuda_fail(e_, #call);      \
+    } while (0)
+
+struct DevCtx {
+    bool ready = false;
+    uint32_t* enum_tabs = nullptr;
+    unsigned int* err = nullptr;
+};
+
+std::mutex g_mu;
+DevCtx g_ctx[64];
+std::vector<uint32_t> g_enum_host;
+sg_code_tables g_code;
+bool g_host_ready = false;
+
+const double k_etab_host[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
+const double k_ltab_host[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
+
+sg_status host_init_locked()
+{
+    if (g_host_ready)
+        return SG_OK;
+    sg_code_build(&g_code);
+    g_enum_host.assign((size_t)SG_ENUM_NTAB * SG_ENUM_LEN, 0);
+    for (int ic = 0; ic < SG_ENUM_NTAB; ic++)
+        if (sg_enum_build(ic, g_enum_host.data() + (size_t)ic * SG_ENUM_LEN) != SG_ENUM_LEN)
+            return fail(SG_ERR_ARG, "error-pattern order table incomplete");
+    g_host_ready = true;
+    return SG_OK;
+}
+
+sg_status get_ctx(DevCtx** out)
+{
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64)
+        return fail(SG_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevCtx& c = g_ctx[dev];
+    if (!c.ready) {
+        sg_status s = host_init_locked();
+        if (s != SG_OK)
+            return s;
+        const size_t bytes = g_enum_host.size() * sizeof(uint32_t);
+        SG_CUDA(cudaMalloc(&c.enum_tabs, bytes));
+        SG_CUDA(cudaMemcpy(c.enum_tabs, g_enum_host.data(), bytes, cudaMemcpyHostToDevice));
+        SG_CUDA(cudaMalloc(&c.err, sizeof(unsigned int)));
+        SG_CUDA(cudaMemset(c.err, 0, sizeof(unsigned int)));
+        SG_CUDA(cudaMemcpyToSymbol(c_hcol, g_code.hcol, sizeof g_code.hcol));
+        SG_CUDA(cudaMemcpyToSymbol(c_prow, g_code.prow, sizeof g_code.prow));
+        SG_CUDA(cudaMemcpyToSymbol(c_ptab, g_code.ptab, sizeof g_code.ptab));
+        SG_CUDA(cudaFuncSetAttribute(sg_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(SgCwSmem)));
+        c.ready = true;
+    }
+    *out = &c;
+    return SG_OK;
+}
+
+sg_status check_params(const sg_params* p)
+{
+    if (!p)
+        return fail(SG_ERR_ARG, "params is NULL");
+    if (p->L < 1 || p->L > SG_MAX_L)
+        return fail(SG_ERR_ARG, "L must be in [1, 8]");
+    if (p->Imax < 1 || p->Imax > SG_MAX_IMAX)
+        return fail(SG_ERR_ARG, "Imax must be in [1, 50]");
+    if (!(p->thres == p->thres))
+        return fail(SG_ERR_ARG, "thres is NaN");
+    for (int i = 0; i < 3 * p->Imax; i++)
+        if (!isfinite(p->alpha[i]))
+            return fail(SG_ERR_ARG, "alpha must be finite");
+    return SG_OK;
+}
+
+uint32_t tmax_eff(uint64_t tmax)
+{
+    if (tmax == 0)
+        return 0x7fffffffu; /* if (Tmax==0) Tmax=Inf, :607 */
+    return tmax > 0xffffffffull ? 0xffffffffu : (uint32_t)tmax;
+}
+
+int grid_for(unsigned long long n, int cap)
+{
+    return (int)(n < (unsigned long long)cap ? n : (unsigned long long)cap);
+}
+
+} // namespace
+
+extern "C" {
+
+void sg_params_default(sg_params* p)
+{
+    if (!p)
+        return;
+    memset(p, 0, sizeof *p);
+    p->L = 3;
+    p->Imax = 30;
+    p->Tmax = UINT64_MAX;
+    p->thres = 1.0 - 1e-5;
+    for (int i = 0; i < SG_MAX_PHASES; i++)
+        p->alpha[i] = 0.7;
+}
+
+sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
+                           double* d_lapp, sg_cw_stats* d_stats, void* stream)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (n_cw == 0)
+        return SG_OK;
+    if (!d_llr || !d_bits)
+        return fail(SG_ERR_ARG, "llr and bits must not be NULL");
+    if ((uintptr_t)d_llr & 7u)
+        return fail(SG_ERR_ARG, "llr must be 8-byte aligned");
+    DevCtx* c = nullptr;
+    if ((s = get_ctx(&c)) != SG_OK)
+        return s;
+    SgDecodeArgs a;
+    memset(&a, 0, sizeof a);
+    a.llr = d_llr;
+    a.bits = d_bits;
+    a.lapp = d_lapp;
+    a.stats = d_stats;
+    a.enum_tabs = c->enum_tabs;
+    a.err = c->err;
+    a.n_cw = n_cw;
+    a.L = p->L;
+    a.imax = p->Imax;
+    a.tmax = tmax_eff(p->Tmax);
+    a.use_bulk = ((uintptr_t)d_llr & 15u) == 0;
+    a.thres = p->thres;
+    memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    const int grid = grid_for(n_cw, 1 << 30);
+    sg_decode_kernel<<<grid, SG_THREADS, sizeof(SgCwSmem), (cudaStream_t)stream>>>(a);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+sg_status sg_bitso_device(const double* d_llr, size_t n_lines, int32_t L, uint64_t Tmax, double thres,
+                          double* d_lapp, double* d_le, int32_t* d_nguess, int32_t* d_ncw, void* stream)
+{
+    if (L < 1 || L > SG_MAX_L)
+        return fail(SG_ERR_ARG, "L must be in [1, 8]");
+    if (n_lines == 0)
+        return SG_OK;
+    if (!d_llr || !d_lapp || !d_le || !d_nguess)
+        return fail(SG_ERR_ARG, "NULL buffer");
+    DevCtx* c = nullptr;
+    sg_status s = get_ctx(&c);
+    if (s != SG_OK)
+        return s;
+    SgLineParams lp;
+    lp.L = L;
+    lp.tmax = tmax_eff(Tmax);
+    lp.thres = thres;
+    const unsigned long long blocks = (n_lines + SG_WARPS - 1) / SG_WARPS;
+    sg_bitso_kernel<<<grid_for(blocks, 148 * 64), SG_THREADS, 0, (cudaStream_t)stream>>>(
+        d_llr, n_lines, lp, d_lapp, d_le, d_nguess, d_ncw, c->enum_tabs);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+sg_status sg_bitso_host(const double* llr, size_t n_lines, int32_t L, uint64_t Tmax, double thres,
+                        double* lapp, double* le, int32_t* nguess, int32_t* ncw)
+{
+    if (n_lines == 0)
+        return SG_OK;
+    if (!llr || !lapp || !le || !nguess)
+        return fail(SG_ERR_ARG, "NULL buffer");
+    double *dl = nullptr, *da = nullptr, *de = nullptr;
+    int32_t *dn = nullptr, *dc = nullptr;
+    const size_t vb = n_lines * 16 * sizeof(double), ib = n_lines * sizeof(int32_t);
+    sg_status s = SG_OK;
+    cudaError_t e;
+    if ((e = cudaMalloc(&dl, vb)) != cudaSuccess || (e = cudaMalloc(&da, vb)) != cudaSuccess ||
+        (e = cudaMalloc(&de, vb)) != cudaSuccess || (e = cudaMalloc(&dn, ib)) != cudaSuccess ||
+        (e = cudaMalloc(&dc, ib)) != cudaSuccess) {
+        s = cuda_fail(e, "cudaMalloc");
+    } else if ((e = cudaMemcpy(dl, llr, vb, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        s = cuda_fail(e, "cudaMemcpy H2D");
+    } else if ((s = sg_bitso_device(dl, n_lines, L, Tmax, thres, da, de, dn, dc, nullptr)) == SG_OK) {
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess ||
+            (e = cudaMemcpy(lapp, da, vb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (e = cudaMemcpy(le, de, vb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (e = cudaMemcpy(nguess, dn, ib, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (ncw && (e = cudaMemcpy(ncw, dc, ib, cudaMemcpyDeviceToHost)) != cudaSuccess))
+            s = cuda_fail(e, "bitso copy-out");
+    }
+    cudaFree(dl);
+    cudaFree(da);
+    cudaFree(de);
+    cudaFree(dn);
+    cudaFree(dc);
+    return s;
+}
+
+sg_status sg_decode_host(const double* llr, size_t n_cw, const sg_params* p, uint8_t* bits, double* lapp,
+                         sg_cw_stats* stats)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (n_cw == 0)
+        return SG_OK;
+    if (!llr || !bits)
+        return fail(SG_ERR_ARG, "llr and bits must not be NULL");
+    /* bounded device footprint: chunks of at most 32768 codewords (1 GiB of LLRs) */
+    const size_t chunk = n_cw < 32768 ? n_cw : 32768;
+    double *dl = nullptr, *da = nullptr;
+    uint8_t* db = nullptr;
+    sg_cw_stats* dst = nullptr;
+    std::vector<sg_cw_stats> hst;
+    cudaError_t e;
+    bool any_nonfinite = false;
+    if ((e = cudaMalloc(&dl, chunk * SG_CUBE * sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&db, chunk * SG_INFO_BYTES)) != cudaSuccess ||
+        (e = cudaMalloc(&dst, chunk * sizeof(sg_cw_stats))) != cudaSuccess ||
+        (lapp && (e = cudaMalloc(&da, chunk * SG_CUBE * sizeof(double))) != cudaSuccess)) {
+        s = cuda_fail(e, "cudaMalloc");
+    } else {
+        hst.resize(chunk);
+        for (size_t off = 0; off < n_cw && s == SG_OK; off += chunk) {
+            const size_t n = (n_cw - off) < chunk ? (n_cw - off) : chunk;
+            if ((e = cudaMemcpy(dl, llr + off * SG_CUBE, n * SG_CUBE * sizeof(double), cudaMemcpyHostToDevice)) !=
+                cudaSuccess) {
+                s = cuda_fail(e, "cudaMemcpy H2D");
+                break;
+            }
+            if ((s = sg_decode_device(dl, n, p, db, da, dst, nullptr)) != SG_OK)
+                break;
+            if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+                s = cuda_fail(e, "decode");
+                break;
+            }
+            if ((e = cudaMemcpy(bits + off * SG_INFO_BYTES, db, n * SG_INFO_BYTES, cudaMemcpyDeviceToHost)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpy(hst.data(), dst, n * sizeof(sg_cw_stats), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+                (lapp && (e = cudaMemcpy(lapp + off * SG_CUBE, da, n * SG_CUBE * sizeof(double),
+                                         cudaMemcpyDeviceToHost)) != cudaSuccess)) {
+                s = cuda_fail(e, "cudaMemcpy D2H");
+                break;
+            }
+            for (size_t i = 0; i < n; i++)
+                any_nonfinite |= hst[i].converged < 0;
+            {
+                DevCtx* c = nullptr;
+                unsigned int herr = 0;
+                if ((s = get_ctx(&c)) != SG_OK)
+                    break;
+                if ((e = cudaMemcpy(&herr, c->err, sizeof herr, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+                    s = cuda_fail(e, "error flag");
+                    break;
+                }
+                if (herr) {
+                    cudaMemset(c->err, 0, sizeof herr);
+                    s = fail(SG_ERR_TIMEOUT, "a bulk copy into shared memory did not complete");
+                    break;
+                }
+            }
+            if (stats)
+                memcpy(stats + off, hst.data(), n * sizeof(sg_cw_stats));
+        }
+    }
+    cudaFree(dl);
+    cudaFree(db);
+    cudaFree(dst);
+    cudaFree(da);
+    if (s == SG_OK && any_nonfinite)
+        return fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
+    return s;
+}
+
+sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_params* p, size_t chunk_cw,
+                         sg_run_summary* summary)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (!in_path || !out_path)
+        return fail(SG_ERR_ARG, "NULL path");
+    const auto t0 = std::chrono::steady_clock::now();
+    FILE* fi = fopen(in_path, "rb");
+    if (!fi)
+        return fail(SG_ERR_IO, std::string("Error opening input file: ") + strerror(errno));
+    FILE* fo = fopen(out_path, "wb");
+    if (!fo) {
+        fclose(fi);
+        return fail(SG_ERR_IO, std::string("Error opening output file: ") + strerror(errno));
+    }
+    if (chunk_cw == 0)
+        chunk_cw = 16384;
+    std::vector<double> buf(chunk_cw * SG_CUBE);
+    std::vector<uint8_t> bits(chunk_cw * SG_INFO_BYTES);
+    std::vector<sg_cw_stats> st(chunk_cw);
+    sg_run_summary sum;
+    memset(&sum, 0, sizeof sum);
+    for (;;) {
+        const size_t got = fread(buf.data(), sizeof(double) * SG_CUBE, chunk_cw, fi);
+        if (got == 0)
+            break;
+        s = sg_decode_host(buf.data(), got, p, bits.data(), nullptr, st.data());
+        if (s != SG_OK)
+            break;
+        if (fwrite(bits.data(), SG_INFO_BYTES, got, fo) != got) {
+            s = fail(SG_ERR_IO, "short write to output file");
+            break;
+        }
+        for (size_t i = 0; i < got; i++) {
+            sum.total_iterations += st[i].iterations;
+            sum.total_ng += st[i].ng;
+            sum.total_ng_p += st[i].ng_p;
+        }
+        sum.blocks += got;
+        if (got < chunk_cw)
+            break;
+    }
+    if (s == SG_OK && ferror(fi))
+        s = fail(SG_ERR_IO, "read error on input file");
+    fclose(fi);
+    if (fclose(fo) != 0 && s == SG_OK)
+        s = fail(SG_ERR_IO, "error closing output file");
+    sum.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (summary)
+        *summary = sum;
+    return s;
+}
+
+double sg_channel_sigma(double ebn0_db)
+{
+    const int n = 16, k = 8;
+    const double R = pow((double)k / n, 3);
+    const double es = ebn0_db + 10 * log10(2 * R);
+    return 1.0 / sqrt(pow(10, es / 10.0));
+}
+
+sg_status sg_gen_info_host(uint64_t seed, uint64_t cw0, size_t n_cw, uint8_t* info)
+{
+    if (!info && n_cw)
+        return fail(SG_ERR_ARG, "info is NULL");
+    for (size_t c = 0; c < n_cw; c++)
+        for (int w = 0; w < 8; w++) {
+            const uint64_t r = sg_rand(seed, 0, (cw0 + c) * 8 + w);
+            for (int q = 0; q < 8; q++)
+                info[c * SG_INFO_BYTES + w * 8 + q] = (uint8_t)(r >> (8 * q));
+        }
+    return SG_OK;
+}
+
+sg_status sg_encode_host(const uint8_t* info, size_t n_cw, uint8_t* code_bits)
+{
+    if ((!info || !code_bits) && n_cw)
+        return fail(SG_ERR_ARG, "NULL buffer");
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        sg_status s = host_init_locked();
+        if (s != SG_OK)
+            return s;
+    }
+    uint16_t W[256];
+    for (size_t c = 0; c < n_cw; c++) {
+        sg_encode_words(info + c * SG_INFO_BYTES, g_code.prow, g_code.ptab, W);
+        for (int p = 0; p < SG_CUBE; p++)
+            code_bits[c * SG_CUBE + p] = (uint8_t)((W[p >> 4] >> (p & 15)) & 1);
+    }
+    return SG_OK;
+}
+
+sg_status sg_gen_llr_host(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma, double ebn0_lo_db,
+                          double ebn0_hi_db, uint8_t* info, double* llr)
+{
+    if (!llr && n_cw)
+        return fail(SG_ERR_ARG, "llr is NULL");
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        sg_status s = host_init_locked();
+        if (s != SG_OK)
+            return s;
+    }
+    uint8_t ib[SG_INFO_BYTES];
+    uint16_t W[256];
+    for (size_t c = 0; c < n_cw; c++) {
+        const uint64_t gc = cw0 + c;
+        sg_gen_info_host(seed, gc, 1, ib);
+        if (info)
+            memcpy(info + c * SG_INFO_BYTES, ib, SG_INFO_BYTES);
+        sg_encode_words(ib, g_code.prow, g_code.ptab, W);
+        const double s = sigma > 0.0 ? sigma : sg_sigma_draw(seed, gc, ebn0_lo_db, ebn0_hi_db, k_etab_host);
+        for (int p = 0; p < SG_CUBE; p++) {
+            const int bit = (W[p >> 4] >> (p & 15)) & 1;
+            llr[c * SG_CUBE + p] = sg_llr_of(bit, s, sg_normal(seed, gc, (uint32_t)p, k_ltab_host));
+        }
+    }
+    return SG_OK;
+}
+
+sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma, double ebn0_lo_db,
+                            double ebn0_hi_db, uint8_t* d_info, double* d_llr, void* stream)
+{
+    if (n_cw == 0)
+        return SG_OK;
+    if (!d_llr)
+        return fail(SG_ERR_ARG, "llr is NULL");
+    DevCtx* c = nullptr;
+    sg_status s = get_ctx(&c);
+    if (s != SG_OK)
+        return s;
+    sg_gen_kernel<<<grid_for(n_cw, 148 * 16), SG_THREADS, 0, (cudaStream_t)stream>>>(
+        seed, cw0, n_cw, sigma, ebn0_lo_db, ebn0_hi_db, d_info, d_llr);
+    SG_CUDA(cudaGetLastError());
+    return SG_OK;
+}
+
+size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
+{
+    if (ic < 0 || !out)
+        return 0;
+    std::vector<uint32_t> t(SG_ENUM_LEN);
+    const size_t n = sg_enum_build(ic, t.data());
+    const size_t m = n < cap ? n : cap;
+    memcpy(out, t.data(), m * sizeof(uint32_t));
+    return m;
+}
+
+const char* sg_status_string(sg_status s)
+{
+    switch (s) {
+    case SG_OK: return "ok";
+    case SG_ERR_ARG: return "invalid argument";
+    case SG_ERR_CUDA: return "CUDA error";
+    case SG_ERR_NONFINITE: return "non-finite input";
+    case SG_ERR_IO: return "I/O error";
+    case SG_ERR_NOMEM: return "out of memory";
+    case SG_ERR_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+const char* sg_last_error(void) { return t_err.c_str(); }
+
+const char* sg_version(void) { return "sogrand_b200 0.1.0 (sm_100a)"; }
+
+} // extern "C"

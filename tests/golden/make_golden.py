@@ -1,0 +1,227 @@
+"""Generate the golden fixtures of the parity tests.
+
+Run from the repository root (needs the reference sources, so it runs where
+the reference is available, not on the GPU machine):
+
+    make -C oracle all ref && make -C sogrand_b200/csrc
+    python tests/golden/make_golden.py
+
+Inputs are the seeded synthetic channel outputs of sogrand_b200.gen_llr
+(regenerated bit-identically at test time and checked against the SHA-256
+recorded here).  Expected outputs come from
+  - the unmodified reference SOGRAND_C/cubic_decoder_final.c, through
+    oracle/_ref/libsgref.so (reference functions + a per-codeword driver) and,
+    for the main fixture, through the unmodified flow binary
+    oracle/_ref/cubic_decoder_final (decoded file and printed averages);
+  - the twin oracle oracle/libsg_oracle_twin.so: the same algorithm with the
+    decoder's own exp/log, whose soft values the CUDA kernel must reproduce
+    bit for bit.
+Writes tests/golden/golden.json and tests/golden/kat_lines.npz.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import json
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libsgref.so")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final")
+TWIN_SO = os.path.join(ROOT, "oracle", "libsg_oracle_twin.so")
+OUT_DIR = os.path.join(ROOT, "tests", "golden")
+UINT64_MAX = (1 << 64) - 1
+THRES = 1.0 - 1e-5
+
+# (name, seed, n_cw, ebn0 dB or (lo, hi), Tmax)
+SETS = [
+    ("cfg1_2dB_100", 20261203, 100, 2.0, UINT64_MAX),
+    ("snr_1.0dB", 101, 24, 1.0, UINT64_MAX),
+    ("snr_1.5dB", 102, 24, 1.5, UINT64_MAX),
+    ("snr_2.5dB", 103, 24, 2.5, UINT64_MAX),
+    ("snr_3.0dB", 104, 24, 3.0, UINT64_MAX),
+    ("mixed_1to3dB", 105, 24, (1.0, 3.0), UINT64_MAX),
+]
+
+
+def sha(b: bytes) -> str:
+    return hashlib.sha256(b).hexdigest()
+
+
+def gen(seed, n, snr):
+    import sogrand_b200 as sg
+
+    if isinstance(snr, tuple):
+        return sg.gen_llr(seed, 0, n, ebn0_range=snr)
+    return sg.gen_llr(seed, 0, n, ebn0_db=snr)
+
+
+class Params(C.Structure):
+    _fields_ = [("L", C.c_int), ("Imax", C.c_int), ("Tmax", C.c_uint64), ("thres", C.c_double),
+                ("alpha", C.c_double * 150)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_double), ("ng", C.c_uint64), ("ng_p", C.c_uint64),
+                ("converged", C.c_int), ("phases", C.c_int)]
+
+
+def ref_one(args):
+    """Reference decode of one codeword -> (bits, iters, ng, ngp, conv, lapp sha)."""
+    llr, tmax = args
+    lib = C.CDLL(REF_SO)
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+    u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
+    u64 = np.ctypeslib.ndpointer(np.uint64, flags="C")
+    i32 = np.ctypeslib.ndpointer(np.int32, flags="C")
+    lib.sgref_decode.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp, u8, dp, dp,
+                                 u64, u64, i32]
+    bits = np.zeros(64, np.uint8)
+    lapp = np.zeros(4096)
+    it = np.zeros(1)
+    ng = np.zeros(1, np.uint64)
+    ngp = np.zeros(1, np.uint64)
+    cv = np.zeros(1, np.int32)
+    lib.sgref_decode(np.ascontiguousarray(llr), 1, 3, 30, tmax, THRES, np.full(100, 0.7), bits, lapp, it, ng,
+                     ngp, cv)
+    return bits.tobytes().hex(), float(it[0]), int(ng[0]), int(ngp[0]), int(cv[0]), sha(lapp.tobytes())
+
+
+def twin_one(args):
+    llr, tmax = args
+    lib = C.CDLL(TWIN_SO)
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+    u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
+    lib.sgo_default_params.argtypes = [C.POINTER(Params)]
+    lib.sgo_decode.argtypes = [dp, C.c_size_t, C.POINTER(Params), u8, dp, C.POINTER(Stats)]
+    p = Params()
+    lib.sgo_default_params(C.byref(p))
+    p.Tmax = tmax
+    st = (Stats * 1)()
+    bits = np.zeros(64, np.uint8)
+    lapp = np.zeros(4096)
+    lib.sgo_decode(np.ascontiguousarray(llr), 1, C.byref(p), bits, lapp, st)
+    s = st[0]
+    return bits.tobytes().hex(), s.iterations, int(s.ng), int(s.ng_p), int(s.converged), sha(lapp.tobytes())
+
+
+def kat_lines(rng, cubes):
+    """Per-line inputs: slices of decoded-looking cubes at several scales plus
+    constructed edge cases (ties, equal magnitudes, zeros, large IC)."""
+    lines = []
+    n = cubes.shape[0]
+    for _ in range(384):
+        c = rng.integers(0, n)
+        b = rng.integers(0, 4096 - 16)
+        lines.append(cubes[c, b:b + 16] * rng.choice([0.5, 1.0, 2.0, 4.0, 8.0, 16.0]))
+    # exact ties between magnitudes (the reference's sort order decides)
+    for _ in range(48):
+        v = rng.normal(0, 2, 16)
+        k = rng.integers(2, 8)
+        idx = rng.choice(16, k, replace=False)
+        v[idx] = np.abs(v[idx[0]]) * rng.choice([-1, 1], k)
+        lines.append(v)
+    # all magnitudes equal (beta = 0 -> IC = 0 through the int cast)
+    for _ in range(16):
+        lines.append(rng.choice([-1, 1], 16) * rng.uniform(0.1, 5))
+    # exact zeros (hard decision 1, |L| = 0)
+    for _ in range(16):
+        v = rng.normal(0, 1.5, 16)
+        v[rng.choice(16, rng.integers(1, 5), replace=False)] = 0.0
+        lines.append(v)
+    # nearly equal small magnitudes -> large IC
+    for _ in range(32):
+        v = rng.choice([-1, 1], 16) * (rng.uniform(5, 30) + rng.uniform(0, 1e-3, 16) * rng.choice([1, 100], 16))
+        lines.append(v)
+    # very reliable lines (P_notGuess cancels to ~0)
+    for _ in range(16):
+        lines.append(rng.choice([-1, 1], 16) * rng.uniform(20, 60, 16))
+    return np.ascontiguousarray(np.array(lines, dtype=np.float64))
+
+
+def main():
+    for f in (REF_SO, REF_BIN, TWIN_SO):
+        if not os.path.exists(f):
+            sys.exit(f"missing {f}: run `make -C oracle all ref` first")
+    golden = {"generator": "sogrand_b200.gen_llr (splitmix counter RNG, polar Gaussian, sg_log)",
+              "thres": THRES, "L": 3, "Imax": 30, "sets": {}}
+    ctx = mp.get_context("spawn")
+    t0 = time.time()
+    with ctx.Pool(os.cpu_count()) as pool:
+        for name, seed, n, snr, tmax in SETS:
+            info, llr = gen(seed, n, snr)
+            jobs = [(llr[i], tmax) for i in range(n)]
+            ref = pool.map(ref_one, jobs)
+            twin = pool.map(twin_one, jobs)
+            entry = {
+                "seed": seed, "n_cw": n, "ebn0_db": snr, "Tmax": tmax,
+                "llr_sha256": sha(llr.tobytes()), "info_sha256": sha(info.tobytes()),
+                "ref": {"bits": [r[0] for r in ref], "iterations": [r[1] for r in ref],
+                        "ng": [r[2] for r in ref], "ng_p": [r[3] for r in ref],
+                        "converged": [r[4] for r in ref], "lapp_sha256": [r[5] for r in ref]},
+                "twin": {"bits": [r[0] for r in twin], "iterations": [r[1] for r in twin],
+                         "ng": [r[2] for r in twin], "ng_p": [r[3] for r in twin],
+                         "converged": [r[4] for r in twin], "lapp_sha256": [r[5] for r in twin]},
+            }
+            mism = sum(1 for a, b in zip(ref, twin) if a[:5] != b[:5])
+            entry["ref_vs_twin_discrete_mismatches"] = mism
+            ber = np.mean(np.unpackbits(np.frombuffer(b"".join(bytes.fromhex(r[0]) for r in ref), np.uint8))
+                          != np.unpackbits(info.ravel()))
+            entry["ref_ber"] = float(ber)
+            golden["sets"][name] = entry
+            print(f"{name}: {n} cw, ref-vs-twin discrete mismatches {mism}, BER {ber:.3g}, "
+                  f"avg it {np.mean([r[1] for r in ref]):.2f}, {time.time() - t0:.0f}s", flush=True)
+
+    # the unmodified flow binary on the main fixture: decoded file + averages
+    name, seed, n, snr, _ = SETS[0]
+    _, llr = gen(seed, n, snr)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "llr.bin"), os.path.join(td, "dec.bin")
+        llr.tofile(fin)
+        out = subprocess.run([REF_BIN, fin, fout], check=True, capture_output=True, text=True).stdout
+        dec = open(fout, "rb").read()
+    e = golden["sets"][name]
+    assert dec == b"".join(bytes.fromhex(b) for b in e["ref"]["bits"]), "flow binary bits differ from harness"
+    lines = {l.split(":")[0]: l.split(":")[1].strip() for l in out.splitlines() if ":" in l}
+    assert lines["Average NG per block"] == "%.2f" % (sum(e["ref"]["ng"]) / n)
+    assert lines["Average iterations per block"] == "%.2f" % (sum(e["ref"]["iterations"]) / n)
+    assert lines["Average NG_p per block"] == "%.2f" % (sum(e["ref"]["ng_p"]) / n)
+    e["flow_binary_stdout"] = [l for l in out.splitlines() if not l.startswith("Total CPU time")]
+    print("flow binary agrees with the harness on", name)
+
+    # per-line known answers
+    rng = np.random.default_rng(7)
+    _, cubes = gen(SETS[1][1], 8, SETS[1][3])
+    lines = kat_lines(rng, cubes)
+    ref = C.CDLL(REF_SO)
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+    ref.sgref_bitso.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, dp, dp, C.POINTER(C.c_int)]
+    kat = {"llr": lines}
+    for L, tmax, tag in ((3, UINT64_MAX, "L3"), (1, UINT64_MAX, "L1"), (4, UINT64_MAX, "L4")):
+        lapp = np.zeros_like(lines)
+        le = np.zeros_like(lines)
+        ng = np.zeros(len(lines), np.int32)
+        for i in range(len(lines)):
+            a = np.zeros(16)
+            b = np.zeros(16)
+            k = C.c_int()
+            ref.sgref_bitso(lines[i], L, tmax, THRES, a, b, C.byref(k))
+            lapp[i], le[i], ng[i] = a, b, k.value
+        kat[f"{tag}_lapp"], kat[f"{tag}_le"], kat[f"{tag}_nguess"] = lapp, le, ng
+    np.savez_compressed(os.path.join(OUT_DIR, "kat_lines.npz"), **kat)
+    with open(os.path.join(OUT_DIR, "golden.json"), "w") as f:
+        json.dump(golden, f, indent=1)
+    print("wrote golden.json and kat_lines.npz in %.0fs" % (time.time() - t0))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+"""GPU parity: the CUDA decoder, called through the C ABI, against
+  - the reference (golden fixtures of the unmodified C decoder): decoded
+    bits, per-codeword iterations, NG and NG_p;
+  - the twin oracle (reference algorithm, the kernel's exp/log): everything
+    bit for bit, including the final L_APP bytes.
+The reference and the twin differ only where glibc's exp/log round
+differently from the kernel's (both within 1 ulp); the fixtures record those
+codewords, and the kernel must reproduce the twin there."""
+import hashlib
+import multiprocessing as mp
+
+import numpy as np
+import pytest
+
+from oracle_api import UINT64_MAX, Oracle, twin_decode_one
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(sg, e):
+    snr = e["ebn0_db"]
+    if isinstance(snr, list):
+        return sg.gen_llr(e["seed"], 0, e["n_cw"], ebn0_range=tuple(snr))
+    return sg.gen_llr(e["seed"], 0, e["n_cw"], ebn0_db=snr)
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", ["cfg1_2dB_100", "snr_1.0dB", "snr_1.5dB", "snr_2.5dB", "snr_3.0dB",
+                                  "mixed_1to3dB"])
+def test_decode_matches_twin_and_reference(cuda, sg, golden, name):
+    e = golden["sets"][name]
+    info, llr = _inputs(sg, e)
+    assert _sha(llr) == e["llr_sha256"]
+    bits, stats, lapp = sg.decode(llr, want_lapp=True)
+    n = e["n_cw"]
+    t, r = e["twin"], e["ref"]
+    for i in range(n):
+        # the twin: bit for bit
+        assert bits[i].tobytes().hex() == t["bits"][i], (name, i)
+        assert stats["iterations"][i] == t["iterations"][i], (name, i)
+        assert int(stats["ng"][i]) == t["ng"][i], (name, i)
+        assert int(stats["ng_p"][i]) == t["ng_p"][i], (name, i)
+        assert int(stats["converged"][i]) == t["converged"][i], (name, i)
+        assert _sha(lapp[i]) == t["lapp_sha256"][i], (name, i)
+    # the reference: every codeword the twin reproduces must match exactly
+    same = [i for i in range(n) if (r["bits"][i], r["iterations"][i], r["ng"][i], r["ng_p"][i])
+            == (t["bits"][i], t["iterations"][i], t["ng"][i], t["ng_p"][i])]
+    assert len(same) == n - e["ref_vs_twin_discrete_mismatches"]
+    for i in same:
+        assert bits[i].tobytes().hex() == r["bits"][i]
+        assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i])) == \
+            (r["iterations"][i], r["ng"][i], r["ng_p"][i])
+
+
+def test_config1_bits_and_iterations_equal_reference(cuda, sg, golden):
+    """Config 1 (100 cw, 2 dB): hard bits and iteration counts of every
+    codeword equal the reference's; NG/NG_p equal on every codeword but the
+    recorded libm-rounding ones."""
+    e = golden["sets"]["cfg1_2dB_100"]
+    _, llr = _inputs(sg, e)
+    bits, stats, _ = sg.decode(llr)
+    r = e["ref"]
+    assert [b.tobytes().hex() for b in bits] == r["bits"]
+    assert list(stats["iterations"]) == r["iterations"]
+    ng_diff = [i for i in range(100) if int(stats["ng"][i]) != r["ng"][i]]
+    assert len(ng_diff) == e["ref_vs_twin_discrete_mismatches"]
+
+
+@pytest.mark.parametrize("tag,L", [("L3", 3), ("L1", 1), ("L4", 4)])
+def test_line_kats(cuda, sg, kat, oracle_paths, tag, L):
+    """SOGRAND_bitSO on 528 lines (incl. ties, zeros, equal magnitudes, huge
+    IC, saturated reliabilities): guess counts and signs equal the reference;
+    soft values equal the twin bit for bit."""
+    lapp, le, ng, _ = sg.bitso(kat["llr"], L=L)
+    assert np.array_equal(ng, kat[f"{tag}_nguess"])
+    assert np.array_equal(lapp > 0, kat[f"{tag}_lapp"] > 0)
+    tl, te, tn, _ = Oracle(oracle_paths["twin"]).bitso(kat["llr"], L=L)
+    assert np.array_equal(ng, tn)
+    assert np.array_equal(lapp.view(np.int64), tl.view(np.int64))
+    assert np.array_equal(le.view(np.int64), te.view(np.int64))
+    err = np.abs(lapp - kat[f"{tag}_lapp"])
+    print(f"{tag}: max |L_APP - reference| = {err.max():.3g}")
+
+
+@pytest.mark.parametrize("tmax", [1, 2, 10, 100, 1000, 0])
+def test_line_tmax_cap(cuda, sg, kat, oracle_paths, tmax):
+    """Tmax abandonment (checked once per logistic weight), including lines
+    that find no codeword (curL = 0 branch) and Tmax = 0 (= unlimited)."""
+    lapp, le, ng, nc = sg.bitso(kat["llr"], Tmax=tmax)
+    tl, te, tn, tc = Oracle(oracle_paths["twin"]).bitso(kat["llr"], Tmax=tmax)
+    assert np.array_equal(ng, tn) and np.array_equal(nc, tc)
+    assert np.array_equal(lapp.view(np.int64), tl.view(np.int64))
+    assert np.array_equal(le.view(np.int64), te.view(np.int64))
+
+
+@pytest.mark.parametrize("kw", [dict(Tmax=1000), dict(L=2), dict(L=1, Imax=4), dict(Imax=2),
+                                dict(alpha="ramp"), dict(thres=0.999)])
+def test_decode_variants_match_twin(cuda, sg, oracle_paths, kw):
+    kw = dict(kw)
+    if kw.get("alpha") == "ramp":
+        kw["alpha"] = list(np.linspace(0.3, 1.0, 150))
+    _, llr = sg.gen_llr(424242, 0, 3, ebn0_db=1.75)
+    with mp.get_context("spawn").Pool(3) as pool:
+        ref = pool.map(twin_decode_one, [(oracle_paths["twin"], llr[i], kw) for i in range(3)])
+    bits, stats, lapp = sg.decode(llr, sg.params(**kw), want_lapp=True)
+    for i, (tb, ts, tl) in enumerate(ref):
+        assert np.array_equal(bits[i], tb)
+        assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i]),
+                int(stats["converged"][i]), int(stats["phases"][i])) == ts
+        assert np.array_equal(lapp[i].view(np.int64), tl.view(np.int64))

@@ -1,0 +1,120 @@
+"""GPU properties at scale and edge cases of the C ABI (size-independent
+checks: round trips, batching invariance, determinism, error paths)."""
+import ctypes as C
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+
+def test_noiseless_round_trip_at_scale(cuda, sg):
+    """encode -> BPSK without noise -> decode: every codeword stops after the
+    first phase with the hard decision as its only guess per line."""
+    torch = cuda
+    n = 20000
+    info = sg.gen_info(31, 0, n)
+    cw = sg.encode(info)
+    llr = torch.from_numpy(np.where(cw == 0, 3.0, -3.0)).cuda()
+    bits, raw, _ = sg.decode(llr)
+    torch.cuda.synchronize()
+    st = sg.stats_from_device(raw)
+    assert np.array_equal(bits.cpu().numpy(), info)
+    assert np.all(st["iterations"] == 0.5) and np.all(st["ng"] == 256) and np.all(st["converged"] == 1)
+
+
+def test_device_generator_equals_host(cuda, sg):
+    torch = cuda
+    for kw in (dict(ebn0_db=2.0), dict(ebn0_range=(1.0, 3.0))):
+        hi, hl = sg.gen_llr(99, 1000, 48, **kw)
+        di, dl = sg.gen_llr(99, 1000, 48, device="cuda", **kw)
+        torch.cuda.synchronize()
+        assert np.array_equal(di.cpu().numpy(), hi)
+        assert np.array_equal(dl.cpu().numpy().view(np.int64), hl.view(np.int64))
+
+
+def test_device_api_equals_host_api_and_batching(cuda, sg):
+    torch = cuda
+    _, llr = sg.gen_llr(7, 0, 24, ebn0_db=1.5)
+    hb, hs, hl = sg.decode(llr, want_lapp=True)
+    db, draw, dl = sg.decode(torch.from_numpy(llr).cuda(), want_lapp=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(db.cpu().numpy(), hb)
+    assert np.array_equal(sg.stats_from_device(draw), hs)
+    assert np.array_equal(dl.cpu().numpy().view(np.int64), hl.view(np.int64))
+    # any sub-batch decodes the same codewords identically
+    for a, b in ((0, 1), (5, 17), (23, 24)):
+        sb, ss, _ = sg.decode(llr[a:b])
+        assert np.array_equal(sb, hb[a:b]) and np.array_equal(ss, hs[a:b])
+
+
+def test_unaligned_input_uses_plain_loads(cuda, sg):
+    """A cube pointer that is 8- but not 16-byte aligned takes the plain-load
+    path and gives the same result."""
+    torch = cuda
+    _, llr = sg.gen_llr(8, 0, 4, ebn0_db=2.0)
+    buf = torch.zeros(4 * 4096 + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(llr.ravel()).cuda()
+    view = buf[1:]
+    assert view.data_ptr() % 16 == 8
+    b1, s1, _ = sg.decode(view)
+    b2, s2, _ = sg.decode(torch.from_numpy(llr).cuda())
+    torch.cuda.synchronize()
+    assert torch.equal(b1, b2) and torch.equal(s1, s2)
+
+
+def test_nonfinite_codeword_is_reported(cuda, sg):
+    _, llr = sg.gen_llr(9, 0, 3, ebn0_db=2.5)
+    good_b, good_s, _ = sg.decode(llr)
+    bad = llr.copy()
+    bad[1, 777] = np.nan
+    with pytest.raises(sg.SograndError) as e:
+        sg.decode(bad)
+    assert e.value.status == 3
+    from sogrand_b200 import _lib
+
+    lib = _lib.load()
+    bits = np.zeros((3, 64), np.uint8)
+    st = np.zeros(3, sg.STATS_DTYPE)
+    p = sg.params()
+    r = lib.sg_decode_host(bad.ctypes.data, 3, C.byref(p), bits.ctypes.data, None, st.ctypes.data)
+    assert r == 3
+    assert st["converged"][1] == -1 and np.all(bits[1] == 0)
+    for i in (0, 2):
+        assert np.array_equal(bits[i], good_b[i]) and st[i] == good_s[i]
+
+
+def test_determinism_and_stats_at_scale(cuda, sg):
+    torch = cuda
+    n = 4096
+    _, llr = sg.gen_llr(2026, 0, n, ebn0_db=2.0, device="cuda")
+    b1, s1, _ = sg.decode(llr)
+    b2, s2, _ = sg.decode(llr)
+    torch.cuda.synchronize()
+    assert torch.equal(b1, b2) and torch.equal(s1, s2)
+    st = sg.stats_from_device(s1)
+    assert 4.0 < st["iterations"].mean() < 6.0
+    assert 1.6e6 < st["ng"].mean() < 2.4e6
+    assert (st["converged"] == 1).mean() > 0.99
+
+
+def test_cli_drop_in(cuda, sg, tmp_path):
+    """The cubic_decoder CLI: same argv, files and statistics lines as the
+    reference decoder process."""
+    info, llr = sg.gen_llr(5, 0, 6, ebn0_db=2.0)
+    llr.tofile(tmp_path / "llr.bin")
+    exe = os.path.join(ROOT, "sogrand_b200", "bin", "cubic_decoder")
+    out = subprocess.run([exe, str(tmp_path / "llr.bin"), str(tmp_path / "dec.bin")], check=True,
+                         capture_output=True, text=True).stdout.splitlines()
+    bits, st, _ = sg.decode(llr)
+    assert (tmp_path / "dec.bin").read_bytes() == bits.tobytes()
+    assert out[0] == "Decoding complete. 6 block(s) decoded."
+    assert out[1] == "Average iterations per block: %.2f" % st["iterations"].mean()
+    assert out[2] == "Average NG per block: %.2f" % (st["ng"].sum() / 6)
+    assert out[4] == "Average NG_p per block: %.2f" % (st["ng_p"].sum() / 6)
+    assert out[-1].startswith("Throughput: ")
