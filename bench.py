@@ -193,6 +193,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cw-per-core", type=int, default=16)
     ap.add_argument("--ref-cw-per-core", type=int, default=4)
+    ap.add_argument("--variant", default=None, help="decoder kernel variant (name or index)")
+    ap.add_argument("--autotune", action="store_true", help="measure all variants first, keep the fastest")
     ap.add_argument("--port-worker", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.port_worker:
@@ -218,6 +220,13 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
+    from sogrand_b200 import autotune
+
+    tune = None
+    if args.variant is not None:
+        autotune.set_variant(int(args.variant) if args.variant.isdigit() else args.variant)
+    elif args.autotune:
+        tune = autotune.autotune(device=local)
     # every rank decodes its own codeword range of the same stream (no data-path collective)
     n = args.n_cw
     cw0 = rank * n
@@ -263,27 +272,30 @@ def main():
     ng_per_cw = float(st["ng"].mean())
 
     # end to end through the public C ABI with pinned host buffers
-    llr_h = torch.empty((n, 4096), dtype=torch.float64, pin_memory=True)
-    llr_h.copy_(llr)
-    bits_h = torch.empty((n, 64), dtype=torch.uint8, pin_memory=True)
-    stats_h = np.zeros(n, sg.STATS_DTYPE)
-    del llr
-    torch.cuda.empty_cache()
-    lib.sg_decode_host(llr_h.data_ptr(), n, C.byref(p), bits_h.data_ptr(), None, stats_h.ctypes.data)  # warm
-    if pg:
-        pg.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
+    e2e = None
+    if args.e2e_steps > 0:
+        llr_h = torch.empty((n, 4096), dtype=torch.float64, pin_memory=True)
+        llr_h.copy_(llr)
+        bits_h = torch.empty((n, 64), dtype=torch.uint8, pin_memory=True)
+        stats_h = np.zeros(n, sg.STATS_DTYPE)
+        del llr
+        torch.cuda.empty_cache()
         _lib.check(lib.sg_decode_host(llr_h.data_ptr(), n, C.byref(p), bits_h.data_ptr(), None,
-                                      stats_h.ctypes.data))
-    e2e_dt = (time.perf_counter() - t0) / args.e2e_steps
-    if pg:
-        t = torch.tensor([e2e_dt], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_dt = float(t.item())
-    e2e = {"value": world * n / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": n * 4096 * 8,
-           "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
-           "api": "sg_decode_host (host buffers, copies inside the timed region)"}
+                                      stats_h.ctypes.data))  # warm-up
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            _lib.check(lib.sg_decode_host(llr_h.data_ptr(), n, C.byref(p), bits_h.data_ptr(), None,
+                                          stats_h.ctypes.data))
+        e2e_dt = (time.perf_counter() - t0) / args.e2e_steps
+        if pg:
+            t = torch.tensor([e2e_dt], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_dt = float(t.item())
+        e2e = {"value": world * n / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": n * 4096 * 8,
+               "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
+               "api": "sg_decode_host (host buffers, copies inside the timed region)"}
 
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
@@ -307,6 +319,7 @@ def main():
                          "frac": achieved / hbm_peak, "traffic": None,
                          "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},
             "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+            "variant": autotune.get_variant(), "autotune": tune,
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)

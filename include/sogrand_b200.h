@@ -157,6 +157,15 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
                             double ebn0_lo_db, double ebn0_hi_db, uint8_t* d_info,
                             double* d_llr, void* stream);
 
+/* ---- kernel configuration (process-wide).  Variants differ in warps per
+ * codeword CTA and in where the 32 KB channel cube is held (shared memory,
+ * staged by a bulk asynchronous copy, or global memory through L2); all give
+ * identical results.  sogrand_b200.autotune() measures them. */
+int sg_decoder_variant_count(void);
+const char* sg_decoder_variant_name(int v);
+sg_status sg_decoder_set_variant(int v);
+int sg_decoder_get_variant(void);
+
 /* ---- diagnostics */
 
 /* The order in which a line decode tests error patterns when its

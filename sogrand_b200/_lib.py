@@ -80,6 +80,10 @@ _SIGS = {
         [C.c_uint64, C.c_uint64, C.c_size_t, C.c_double, C.c_double, C.c_double, _VP, _VP, _VP],
     ),
     "sg_pattern_order": (C.c_size_t, [C.c_int32, _VP, C.c_size_t]),
+    "sg_decoder_variant_count": (C.c_int, []),
+    "sg_decoder_variant_name": (C.c_char_p, [C.c_int]),
+    "sg_decoder_set_variant": (C.c_int, [C.c_int]),
+    "sg_decoder_get_variant": (C.c_int, []),
     "sg_status_string": (C.c_char_p, [C.c_int]),
     "sg_last_error": (C.c_char_p, []),
     "sg_version": (C.c_char_p, []),

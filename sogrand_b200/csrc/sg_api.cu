@@ -61,12 +61,16 @@ struct SgDecodeArgs {
     double alpha[SG_MAX_PHASES];
 };
 
+/* Shared memory of a decode CTA.  With LCH_SMEM the channel cube is staged
+ * here by one bulk copy; otherwise each line reads its 16 channel LLRs from
+ * global memory (L2-resident) once per phase. */
+template <int NW, bool LCH_SMEM>
 struct SgCwSmem {
-    double lch[SG_CUBE];
+    double lch[LCH_SMEM ? SG_CUBE : 2];
     double le[SG_CUBE];
     double etab[SG_EXP_TAB_LEN];
     double ltab[SG_LOG_TAB_LEN];
-    SgWarpScratch ws[SG_WARPS];
+    SgWarpScratch ws[NW];
     uint16_t hdw[256];
     unsigned long long mbar;
     unsigned long long ng;
@@ -128,16 +132,19 @@ __device__ __forceinline__ uint32_t sg_smem_u32(const void* p)
 
 extern __shared__ __align__(128) unsigned char sg_smem_raw[];
 
-__global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
+template <int NW, bool LCH_SMEM, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
 {
-    SgCwSmem& S = *reinterpret_cast<SgCwSmem*>(sg_smem_raw);
+    constexpr int NT = NW * 32;
+    SgCwSmem<NW, LCH_SMEM>& S = *reinterpret_cast<SgCwSmem<NW, LCH_SMEM>*>(sg_smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < SG_EXP_TAB_LEN; i += SG_THREADS)
+    const bool use_bulk = LCH_SMEM && args.use_bulk;
+    for (int i = tid; i < SG_EXP_TAB_LEN; i += NT)
         S.etab[i] = g_etab[i];
-    for (int i = tid; i < SG_LOG_TAB_LEN; i += SG_THREADS)
+    for (int i = tid; i < SG_LOG_TAB_LEN; i += NT)
         S.ltab[i] = g_ltab[i];
     const uint32_t mbar = sg_smem_u32(&S.mbar);
-    if (tid == 0 && args.use_bulk) {
+    if (tid == 0 && use_bulk) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -150,7 +157,7 @@ __global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_c
 
     for (unsigned long long cw = blockIdx.x; cw < args.n_cw; cw += gridDim.x) {
         const double* g = args.llr + cw * SG_CUBE;
-        if (args.use_bulk) {
+        if (use_bulk) {
             if (tid == 0) {
                 /* order earlier generic-proxy reads of lch before the async write */
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -163,18 +170,18 @@ __global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_c
                     "l"(g), "r"((uint32_t)(SG_CUBE * 8)), "r"(mbar)
                     : "memory");
             }
-        } else {
-            for (int i = tid; i < SG_CUBE; i += SG_THREADS)
+        } else if (LCH_SMEM) {
+            for (int i = tid; i < SG_CUBE; i += NT)
                 S.lch[i] = g[i];
         }
-        for (int i = tid; i < SG_CUBE; i += SG_THREADS)
+        for (int i = tid; i < SG_CUBE; i += NT)
             S.le[i] = 0.0;
         if (tid == 0) {
             S.ng = 0;
             S.conv = 0;
             S.bad = 0;
         }
-        if (args.use_bulk && tid == 0) {
+        if (use_bulk && tid == 0) {
             uint32_t ok = 0;
             for (long long it = 0; it < SG_SPIN_LIMIT && !ok; it++) {
                 asm volatile(
@@ -193,8 +200,8 @@ __global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_c
         if (S.bad == 2) /* the bulk copy never completed: skip this codeword */
             break;
         bool nonfinite = false;
-        for (int i = tid; i < SG_CUBE; i += SG_THREADS)
-            nonfinite |= !isfinite(S.lch[i]);
+        for (int i = tid; i < SG_CUBE; i += NT)
+            nonfinite |= !isfinite(LCH_SMEM ? S.lch[i] : __ldg(g + i));
         if (__syncthreads_or(nonfinite)) {
             if (tid < SG_INFO_BYTES)
                 args.bits[cw * SG_INFO_BYTES + tid] = 0;
@@ -232,8 +239,8 @@ __global__ void __launch_bounds__(SG_THREADS, 3) sg_decode_kernel(const __grid_c
                         break;
                     const int pos = sg_pos(axis, l, lane & 15);
                     double v = 1.0;
-                    if (lane < 16)
-                        v = __dadd_rn(S.lch[pos], __dmul_rn(alpha, S.le[pos])); /* L_ch + (alpha*L_E) */
+                    if (lane < 16) /* L_ch + (alpha*L_E) */
+                        v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, S.le[pos]));
                     const SgLineResult r =
                         sg_decode_line(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
                     if (lane < 16) {
@@ -385,6 +392,27 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
     }
 }
 
+/* Decoder kernel configurations: warps per codeword CTA, channel cube in
+ * shared memory (bulk copy) or read from global memory, minimum resident
+ * CTAs per SM for the register budget. */
+struct SgVariant {
+    const char* name;
+    int nw;
+    bool lch_smem;
+    size_t smem;
+    const void* fn;
+};
+
+#define SG_VARIANT(NW, L, M, NAME) \
+    { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M> }
+static const SgVariant g_variants[] = {
+    SG_VARIANT(8, false, 3, "w8-gmem"),
+    SG_VARIANT(8, true, 2, "w8-smem"),
+    SG_VARIANT(12, true, 2, "w12-smem"),
+    SG_VARIANT(16, false, 2, "w16-gmem"),
+};
+#define SG_NVARIANTS ((int)(sizeof(g_variants) / sizeof(g_variants[0])))
+
 /* -------------------------------------------------------------- host -- */
 
 namespace {
@@ -416,6 +444,7 @@ struct DevCtx {
 };
 
 std::mutex g_mu;
+int g_variant = 0;
 DevCtx g_ctx[64];
 std::vector<uint32_t> g_enum_host;
 sg_code_tables g_code;
@@ -457,8 +486,9 @@ sg_status get_ctx(DevCtx** out)
         SG_CUDA(cudaMemcpyToSymbol(c_hcol, g_code.hcol, sizeof g_code.hcol));
         SG_CUDA(cudaMemcpyToSymbol(c_prow, g_code.prow, sizeof g_code.prow));
         SG_CUDA(cudaMemcpyToSymbol(c_ptab, g_code.ptab, sizeof g_code.ptab));
-        SG_CUDA(cudaFuncSetAttribute(sg_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(SgCwSmem)));
+        for (int v = 0; v < SG_NVARIANTS; v++)
+            SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_variants[v].smem));
         c.ready = true;
     }
     *out = &c;
@@ -540,9 +570,10 @@ sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
     a.use_bulk = ((uintptr_t)d_llr & 15u) == 0;
     a.thres = p->thres;
     memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    const SgVariant& v = g_variants[g_variant];
     const int grid = grid_for(n_cw, 1 << 30);
-    sg_decode_kernel<<<grid, SG_THREADS, sizeof(SgCwSmem), (cudaStream_t)stream>>>(a);
-    SG_CUDA(cudaGetLastError());
+    void* kargs[] = {(void*)&a};
+    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem, (cudaStream_t)stream));
     return SG_OK;
 }
 
@@ -830,6 +861,23 @@ size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
     memcpy(out, t.data(), m * sizeof(uint32_t));
     return m;
 }
+
+int sg_decoder_variant_count(void) { return SG_NVARIANTS; }
+
+const char* sg_decoder_variant_name(int v)
+{
+    return (v >= 0 && v < SG_NVARIANTS) ? g_variants[v].name : "";
+}
+
+sg_status sg_decoder_set_variant(int v)
+{
+    if (v < 0 || v >= SG_NVARIANTS)
+        return fail(SG_ERR_ARG, "no such decoder variant");
+    g_variant = v;
+    return SG_OK;
+}
+
+int sg_decoder_get_variant(void) { return g_variant; }
 
 const char* sg_status_string(sg_status s)
 {

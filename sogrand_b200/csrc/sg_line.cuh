@@ -2,19 +2,38 @@
  *
  * Restates SOGRAND_bitSO + sogrand_main_logic
  * (SOGRAND_C/cubic_decoder_final.c:521-746) for n = 16, k = 8, even = 0,
- * as warp-cooperative code:
- *   - lanes 0..15 own the 16 positions of the line for the set-up (hard
- *     decision, |LLR|, JacLog terms, sort, IC, per-position PM increments and
- *     syndrome columns) and for the soft output;
- *   - the guess loop runs 32 consecutive patterns of the enumeration order
- *     at once, one per lane: each lane forms its pattern's path metric and
- *     syndrome and evaluates exp(-PM); a ballot finds the codewords; the
- *     running P_notGuess is then advanced in enumeration order, and the list
- *     is updated at each codeword in that order, so the guess count T and
- *     every floating-point sum match the sequential reference exactly.
- * All floating-point operations that the reference performs are issued as
- * separately rounded IEEE operations (the file is built with -fmad=false);
- * exp/log are sg_exp/sg_log.
+ * as warp-cooperative code with results bit-identical to the sequential
+ * reference (given the same exp/log):
+ *
+ *  set-up   lanes 0..15 own the 16 positions: hard decision, |LLR|,
+ *           JacLog terms, the sort (rank sort, or the reference's exact
+ *           quicksort when magnitudes tie), IC, the PM increment and
+ *           syndrome column of each sorted position.  From these the warp
+ *           builds per-line tables:
+ *             A[lo]     PM_HD + the increments of the bits of lo, added in
+ *                       ascending order -- exactly the prefix of getPM's
+ *                       sequential sum (:765) over the 8 least reliable
+ *                       positions;
+ *             synlo/hi  syndrome of each byte of a pattern (ParityCheck,
+ *                       :748-755, is linear), the hard decision's own
+ *                       syndrome folded into synlo.
+ *  guesses  32 consecutive patterns of the order table per step, one per
+ *           lane: PM = A[lo] + increments of the high bits (ascending),
+ *           syndrome = synlo[lo] ^ synhi[hi], e = exp(-PM).
+ *  P_notGuess  the reference subtracts e of every guess in order (:626,
+ *           :672, :712).  Within one binade [2^E, 2^(E+1)) every difference
+ *           rounds to the grid u = 2^(E-52), so fl(P - e) = u*round(M - e/u)
+ *           with M = P/u an integer: the running value is an exact integer
+ *           prefix sum, computed by a warp scan (sums < 2^53 are exact in
+ *           binary64).  A lane whose term is large, whose rounding is a tie,
+ *           or whose result leaves the binade is instead subtracted alone
+ *           with one IEEE subtraction, and the scan restarts after it.  The
+ *           result equals the sequential loop bit for bit.
+ *  list     codewords are taken in lane order; getLConf (:767-774) uses the
+ *           running P_notGuess at each, so T and the list match exactly.
+ *  output   soft output of :536-577 on lanes 0..15.
+ * The file is built with -fmad=false: every floating-point operation the
+ * reference performs is a separately rounded IEEE operation here.
  */
 #pragma once
 #include <stdint.h>
@@ -31,12 +50,14 @@ struct SgLineParams {
 
 /* Per-warp shared scratch of one line decode. */
 struct SgWarpScratch {
-    double delta[16];   /* JacLog(|L|) - JacLog(-|L|) per sorted position */
+    double A[256];      /* PM prefix over the low byte of a pattern */
+    double dhi[8];      /* PM increments of sorted positions 8..15 */
     double qa[16];      /* values for the tie-exact sort */
     double elist[8];    /* exp(-PM) of the listed codewords */
     uint32_t cmask[8];  /* listed codewords, bit i = position i */
     int32_t perm[16];   /* sorted rank -> position */
-    uint32_t hs[16];    /* syndrome column of each sorted position */
+    uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision) */
+    uint8_t synhi[256]; /* syndrome of the high byte */
 };
 
 __constant__ uint8_t c_hcol[16];
@@ -110,6 +131,38 @@ struct SgLineResult {
     int32_t ncw;      /* codewords found (all lanes) */
 };
 
+/* Warp-uniform list state of a line decode. */
+struct SgListState {
+    double pnl;    /* pNL of the last getLConf */
+    int32_t curl;  /* codewords listed */
+};
+
+/* A codeword found at pattern mask `mj` (sorted positions) whose guess left
+ * P_notGuess = P and contributed ej = exp(-PM): list insertion and getLConf
+ * (:674-686, :767-774).  Returns true when the line decode stops. */
+__device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, SgListState& st, const SgLineParams& lp,
+                                            uint32_t hdm, uint32_t mj, double P, double ej, int lane)
+{
+    uint32_t cm = hdm;
+    for (uint32_t mm = mj; mm; mm &= mm - 1u)
+        cm ^= 1u << ws->perm[__ffs(mm) - 1];
+    __syncwarp();
+    if (lane == 0) {
+        ws->elist[st.curl] = ej;
+        ws->cmask[st.curl] = cm;
+    }
+    __syncwarp();
+    double ppos = 0.0;
+    for (int i = 0; i <= st.curl; i++)
+        ppos = __dadd_rn(ppos, ws->elist[i]);
+    const double pneg = __dmul_rn(0x1p-8, P); /* 2^-(n-k) * P_notGuess */
+    st.pnl = pneg;
+    const double den = __dadd_rn(ppos, pneg);
+    const double conf = (den > 1e-40) ? __ddiv_rn(ppos, den) : 1.0;
+    st.curl++;
+    return conf > lp.thres || st.curl == lp.L;
+}
+
 /* Decode one line.  llr: this lane's input LLR (lanes 0..15; others
  * ignored).  enum_tabs: SG_ENUM_NTAB tables of SG_ENUM_LEN entries.
  * etab/ltab: shared-memory copies of the exp/log tables. */
@@ -127,10 +180,6 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     const uint32_t hdm = __ballot_sync(SG_FULL, act && !(llr > 0.0)) & 0xffffu;
     /* JacLog(-|L_i|) for getPM_HD (:617, :764) */
     const double jn = act ? sg_jaclog(-a, etab, ltab) : 0.0;
-    double pmhd = 0.0;
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        pmhd = __dadd_rn(pmhd, __shfl_sync(SG_FULL, jn, i));
 
     /* QuickSort of |L| ascending (:618) */
     int lt = 0, eq = 0;
@@ -153,6 +202,10 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         if (lane == 0)
             sg_quicksort16(ws->qa, ws->perm);
     }
+    double pmhd = 0.0;
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        pmhd = __dadd_rn(pmhd, __shfl_sync(SG_FULL, jn, i));
     __syncwarp();
     const int src = act ? ws->perm[lane] : 0;
     const double as = __shfl_sync(SG_FULL, a, src);
@@ -168,22 +221,64 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
     /* PM increment of each sorted position (getPM, :765) and its syndrome */
     const double jn_src = __shfl_sync(SG_FULL, jn, src);
-    if (act) {
-        ws->delta[lane] = __dsub_rn(sg_jaclog(as, etab, ltab), jn_src);
-        ws->hs[lane] = c_hcol[src];
-    }
+    const double dl = act ? __dsub_rn(sg_jaclog(as, etab, ltab), jn_src) : 0.0;
+    const uint32_t hs = act ? c_hcol[src] : 0u;
     uint32_t s0 = 0;
 #pragma unroll
     for (int i = 0; i < 16; i++)
         if ((hdm >> i) & 1u)
             s0 ^= c_hcol[i];
+
+    /* per-line tables; lane j fills entries j + 32*i, i = 0..7 */
+    {
+        double d[8];
+        uint32_t hl[8], hh[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            d[b] = __shfl_sync(SG_FULL, dl, b);
+            hl[b] = __shfl_sync(SG_FULL, hs, b);
+            hh[b] = __shfl_sync(SG_FULL, hs, 8 + b);
+        }
+        double v0 = pmhd;
+        uint32_t sl = s0, sh = 0;
+#pragma unroll
+        for (int b = 0; b < 5; b++)
+            if ((lane >> b) & 1) {
+                v0 = __dadd_rn(v0, d[b]);
+                sl ^= hl[b];
+                sh ^= hh[b];
+            }
+        const double v1 = __dadd_rn(v0, d[5]);
+        const double v2 = __dadd_rn(v0, d[6]);
+        const double v3 = __dadd_rn(v1, d[6]);
+        ws->A[lane] = v0;
+        ws->A[lane + 32] = v1;
+        ws->A[lane + 64] = v2;
+        ws->A[lane + 96] = v3;
+        ws->A[lane + 128] = __dadd_rn(v0, d[7]);
+        ws->A[lane + 160] = __dadd_rn(v1, d[7]);
+        ws->A[lane + 192] = __dadd_rn(v2, d[7]);
+        ws->A[lane + 224] = __dadd_rn(v3, d[7]);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            uint32_t x = sl, y = sh;
+            if (i & 1) { x ^= hl[5]; y ^= hh[5]; }
+            if (i & 2) { x ^= hl[6]; y ^= hh[6]; }
+            if (i & 4) { x ^= hl[7]; y ^= hh[7]; }
+            ws->synlo[lane + 32 * i] = (uint8_t)x;
+            ws->synhi[lane + 32 * i] = (uint8_t)y;
+        }
+        if (lane >= 8 && lane < 16)
+            ws->dhi[lane - 8] = dl;
+    }
     __syncwarp();
 
     /* Guess loop (:624-744) */
     const uint32_t* tab = enum_tabs + (size_t)itab * SG_ENUM_LEN;
-    double P = 1.0;   /* P_notGuess */
-    double pnl = 0.0; /* pNL of the last getLConf */
-    int32_t curl = 0;
+    double P = 1.0; /* P_notGuess */
+    SgListState st;
+    st.pnl = 0.0;
+    st.curl = 0;
     uint32_t T = 0;
     bool done = false;
     for (uint32_t base = 0; !done; base += 32) {
@@ -196,45 +291,84 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         if (cut)
             lim &= (1u << (__ffs(cut) - 1)) - 1u;
         const int nv = __popc(lim);
-        uint32_t m = ent & 0xffffu;
-        double pm = pmhd;
-        uint32_t syn = s0;
-        while (m) {
-            const int r = __ffs(m) - 1;
-            pm = __dadd_rn(pm, ws->delta[r]);
-            syn ^= ws->hs[r];
-            m &= m - 1u;
+        const uint32_t lo = ent & 0xffu;
+        uint32_t hi = (ent >> 8) & 0xffu;
+        double pm = ws->A[lo];
+        const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
+        while (hi) {
+            pm = __dadd_rn(pm, ws->dhi[__ffs(hi) - 1]);
+            hi &= hi - 1u;
         }
         const double e = sg_exp(-pm, etab);
         const uint32_t hits = __ballot_sync(SG_FULL, syn == 0u) & lim;
-        for (int j = 0; j < nv; j++) {
-            const double ej = __shfl_sync(SG_FULL, e, j);
-            P = __dsub_rn(P, ej);
-            if ((hits >> j) & 1u) {
-                /* list insertion and getLConf (:674-686, :767-774) */
-                const uint32_t mj = __shfl_sync(SG_FULL, ent, j) & 0xffffu;
-                uint32_t cm = hdm;
-                for (uint32_t mm = mj; mm; mm &= mm - 1u)
-                    cm ^= 1u << ws->perm[__ffs(mm) - 1];
-                __syncwarp();
-                if (lane == 0) {
-                    ws->elist[curl] = ej;
-                    ws->cmask[curl] = cm;
+
+        /* advance P_notGuess over lanes [0, nv) and take the codewords in order */
+        int s = 0;
+        while (s < nv && !done) {
+            if (!(P >= 0x1p-970)) { /* zero, negative, tiny or NaN: one lane alone */
+                const double es = __shfl_sync(SG_FULL, e, s);
+                P = __dsub_rn(P, es);
+                if ((hits >> s) & 1u) {
+                    const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
+                    if (sg_list_hit(ws, st, lp, hdm, mj, P, es, lane)) {
+                        T = base + (uint32_t)s + 1u;
+                        done = true;
+                    }
                 }
-                __syncwarp();
-                double ppos = 0.0;
-                for (int i = 0; i <= curl; i++)
-                    ppos = __dadd_rn(ppos, ws->elist[i]);
-                const double pneg = __dmul_rn(0x1p-8, P); /* 2^-(n-k) * P_notGuess */
-                pnl = pneg;
-                const double den = __dadd_rn(ppos, pneg);
-                const double conf = (den > 1e-40) ? __ddiv_rn(ppos, den) : 1.0;
-                curl++;
-                if (conf > lp.thres || curl == lp.L) {
-                    T = base + (uint32_t)j + 1u;
+                s++;
+                continue;
+            }
+            const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
+            const double u = sg_from_bits((uint64_t)(E - 52 + 1023) << 52);
+            const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
+            const double M0 = __dmul_rn(P, iu);
+            const bool mine = lane >= s && lane < nv;
+            const double q = mine ? __dmul_rn(e, iu) : 0.0;
+            const bool big = !(q < 0x1p52);
+            double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52); /* round(q), ties to even */
+            const bool tie = fabs(__dsub_rn(q, d)) == 0.5;
+            if (big)
+                d = 0.0;
+            double S = d;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const double y = __shfl_up_sync(SG_FULL, S, off);
+                if (lane >= off)
+                    S = __dadd_rn(S, y);
+            }
+            const double M = __dsub_rn(M0, S);
+            const uint32_t bm = __ballot_sync(SG_FULL, mine && (big || tie || !(M >= 0x1p52 + 1.0)));
+            const int f = bm ? __ffs(bm) - 1 : nv;
+            uint32_t hseg = hits & (f >= 32 ? SG_FULL : ((1u << f) - 1u)) & ~((1u << s) - 1u);
+            while (hseg) {
+                const int h = __ffs(hseg) - 1;
+                const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
+                const double eh = __shfl_sync(SG_FULL, e, h);
+                const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
+                if (sg_list_hit(ws, st, lp, hdm, mj, Ph, eh, lane)) {
+                    T = base + (uint32_t)h + 1u;
                     done = true;
                     break;
                 }
+                hseg &= hseg - 1u;
+            }
+            if (done)
+                break;
+            if (f > s)
+                P = __dmul_rn(__shfl_sync(SG_FULL, M, f - 1), u);
+            if (f < nv) {
+                const double es = __shfl_sync(SG_FULL, e, f);
+                P = __dsub_rn(P, es);
+                if ((hits >> f) & 1u) {
+                    const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
+                    if (sg_list_hit(ws, st, lp, hdm, mj, P, es, lane)) {
+                        T = base + (uint32_t)f + 1u;
+                        done = true;
+                    }
+                }
+                s = f + 1;
+            } else {
+                s = nv;
             }
         }
         if (!done) {
@@ -247,19 +381,19 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     /* Soft output (:536-577) */
     SgLineResult res;
     res.T = T;
-    res.ncw = curl;
+    res.ncw = st.curl;
     double lapp, le;
-    if (curl == 0) {
+    if (st.curl == 0) {
         lapp = llr;
         le = 0.0;
     } else {
-        const double pnlc = fmax(pnl, 1e-40);
+        const double pnlc = fmax(st.pnl, 1e-40);
         double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, sg_exp(llr, etab)));
         double pp0 = __dsub_rn(1.0, pp1);
         pp1 = fmin(fmax(pp1, 1e-40), 1.0);
         pp0 = fmin(fmax(pp0, 1e-40), 1.0);
         double p1 = 0.0, p0 = 0.0;
-        for (int j = 0; j < curl; j++) {
+        for (int j = 0; j < st.curl; j++) {
             const double c = (double)((ws->cmask[j] >> lane) & 1u);
             const double pj = ws->elist[j];
             p1 = __dadd_rn(p1, __dmul_rn(c, pj));

@@ -14,13 +14,15 @@ pytestmark = pytest.mark.gpu
 
 
 def test_noiseless_round_trip_at_scale(cuda, sg):
-    """encode -> BPSK without noise -> decode: every codeword stops after the
-    first phase with the hard decision as its only guess per line."""
+    """encode -> BPSK without noise -> decode: with |LLR| = 12 every line's
+    hard decision is a codeword whose list confidence already exceeds
+    1 - 1e-5, so every codeword stops after the first phase, one guess per
+    line."""
     torch = cuda
     n = 20000
     info = sg.gen_info(31, 0, n)
     cw = sg.encode(info)
-    llr = torch.from_numpy(np.where(cw == 0, 3.0, -3.0)).cuda()
+    llr = torch.from_numpy(np.where(cw == 0, 12.0, -12.0)).cuda()
     bits, raw, _ = sg.decode(llr)
     torch.cuda.synchronize()
     st = sg.stats_from_device(raw)
