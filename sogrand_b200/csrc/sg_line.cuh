@@ -53,9 +53,8 @@ struct SgWarpScratch {
     double A[256];      /* PM prefix over the low byte of a pattern */
     double dhi[8];      /* PM increments of sorted positions 8..15 */
     double qa[16];      /* values for the tie-exact sort */
-    double elist[8];    /* exp(-PM) of the listed codewords */
-    uint32_t cmask[8];  /* listed codewords, bit i = position i */
     int32_t perm[16];   /* sorted rank -> position */
+    int32_t rank[16];   /* position -> sorted rank */
     uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision) */
     uint8_t synhi[256]; /* syndrome of the high byte */
 };
@@ -131,30 +130,32 @@ struct SgLineResult {
     int32_t ncw;      /* codewords found (all lanes) */
 };
 
-/* Warp-uniform list state of a line decode. */
+/* List state of a line decode.  Lane k < L holds entry k of the list:
+ * my_e = exp(-PM) of the k-th codeword found, my_cm its bits (bit i =
+ * position i).  curl and pnl are warp-uniform. */
 struct SgListState {
-    double pnl;    /* pNL of the last getLConf */
-    int32_t curl;  /* codewords listed */
+    double pnl;     /* pNL of the last getLConf */
+    double my_e;
+    uint32_t my_cm;
+    int32_t curl;   /* codewords listed */
 };
 
 /* A codeword found at pattern mask `mj` (sorted positions) whose guess left
  * P_notGuess = P and contributed ej = exp(-PM): list insertion and getLConf
- * (:674-686, :767-774).  Returns true when the line decode stops. */
-__device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, SgListState& st, const SgLineParams& lp,
-                                            uint32_t hdm, uint32_t mj, double P, double ej, int lane)
+ * (:674-686, :767-774).  myrank: sorted rank of this lane's position (lanes
+ * 0..15).  Returns true when the line decode stops. */
+__device__ __forceinline__ bool sg_list_hit(SgListState& st, const SgLineParams& lp, uint32_t hdm, uint32_t mj,
+                                            double P, double ej, int lane, int myrank)
 {
-    uint32_t cm = hdm;
-    for (uint32_t mm = mj; mm; mm &= mm - 1u)
-        cm ^= 1u << ws->perm[__ffs(mm) - 1];
-    __syncwarp();
-    if (lane == 0) {
-        ws->elist[st.curl] = ej;
-        ws->cmask[st.curl] = cm;
+    /* AddTEP (:761): position i flips when its sorted rank is in the pattern */
+    const uint32_t cm = hdm ^ (__ballot_sync(SG_FULL, lane < 16 && ((mj >> myrank) & 1u)) & 0xffffu);
+    if (lane == st.curl) {
+        st.my_e = ej;
+        st.my_cm = cm;
     }
-    __syncwarp();
     double ppos = 0.0;
     for (int i = 0; i <= st.curl; i++)
-        ppos = __dadd_rn(ppos, ws->elist[i]);
+        ppos = __dadd_rn(ppos, __shfl_sync(SG_FULL, st.my_e, i));
     const double pneg = __dmul_rn(0x1p-8, P); /* 2^-(n-k) * P_notGuess */
     st.pnl = pneg;
     const double den = __dadd_rn(ppos, pneg);
@@ -208,6 +209,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         pmhd = __dadd_rn(pmhd, __shfl_sync(SG_FULL, jn, i));
     __syncwarp();
     const int src = act ? ws->perm[lane] : 0;
+    if (act)
+        ws->rank[src] = lane;
     const double as = __shfl_sync(SG_FULL, a, src);
 
     /* IC (:619-622): beta = (|L|_(7) - |L|_(0)) / 7, IC = max(round(.), 0) */
@@ -223,11 +226,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     const double jn_src = __shfl_sync(SG_FULL, jn, src);
     const double dl = act ? __dsub_rn(sg_jaclog(as, etab, ltab), jn_src) : 0.0;
     const uint32_t hs = act ? c_hcol[src] : 0u;
-    uint32_t s0 = 0;
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        if ((hdm >> i) & 1u)
-            s0 ^= c_hcol[i];
+    /* syndrome of the hard decision */
+    const uint32_t s0 = __reduce_xor_sync(SG_FULL, (act && ((hdm >> lane) & 1u)) ? (uint32_t)c_hcol[lane] : 0u);
 
     /* per-line tables; lane j fills entries j + 32*i, i = 0..7 */
     {
@@ -273,24 +273,32 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     }
     __syncwarp();
 
+    __syncwarp();
+    const int myrank = act ? ws->rank[lane] : 0;
+
     /* Guess loop (:624-744) */
     const uint32_t* tab = enum_tabs + (size_t)itab * SG_ENUM_LEN;
+    const bool has_tmax = lp.tmax < SG_ENUM_LEN;
     double P = 1.0; /* P_notGuess */
     SgListState st;
     st.pnl = 0.0;
+    st.my_e = 0.0;
+    st.my_cm = 0u;
     st.curl = 0;
     uint32_t T = 0;
     bool done = false;
     for (uint32_t base = 0; !done; base += 32) {
         const uint32_t t = base + lane;
-        const bool valid = t < SG_ENUM_LEN;
-        const uint32_t ent = valid ? __ldg(tab + t) : 0u;
-        /* T < Tmax is checked before each new logistic weight (:652) */
-        const uint32_t cut = __ballot_sync(SG_FULL, valid && (ent & SG_ENUM_GS) && t > 0 && t >= lp.tmax);
-        uint32_t lim = __ballot_sync(SG_FULL, valid);
-        if (cut)
-            lim &= (1u << (__ffs(cut) - 1)) - 1u;
-        const int nv = __popc(lim);
+        const uint32_t ent = __ldg(tab + (t < SG_ENUM_LEN ? t : SG_ENUM_LEN - 1u));
+        int nv = base + 32u <= SG_ENUM_LEN ? 32 : (int)(SG_ENUM_LEN - base);
+        if (has_tmax) {
+            /* T < Tmax is checked before each new logistic weight (:652) */
+            const uint32_t cut =
+                __ballot_sync(SG_FULL, lane < nv && (ent & SG_ENUM_GS) && t > 0 && t >= lp.tmax);
+            if (cut)
+                nv = __ffs(cut) - 1;
+        }
+        const uint32_t lim = nv >= 32 ? SG_FULL : ((1u << nv) - 1u);
         const uint32_t lo = ent & 0xffu;
         uint32_t hi = (ent >> 8) & 0xffu;
         double pm = ws->A[lo];
@@ -299,10 +307,35 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             pm = __dadd_rn(pm, ws->dhi[__ffs(hi) - 1]);
             hi &= hi - 1u;
         }
-        const double e = sg_exp(-pm, etab);
+        const double e = sg_exp_neg(-pm, etab);
         const uint32_t hits = __ballot_sync(SG_FULL, syn == 0u) & lim;
 
-        /* advance P_notGuess over lanes [0, nv) and take the codewords in order */
+        /* common case: no codeword, no large term, no tie and no binade
+         * crossing in the batch -- P_notGuess moves by the exact integer sum */
+        if (hits == 0u && P >= 0x1p-970) {
+            const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
+            const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
+            const double q = lane < nv ? __dmul_rn(e, iu) : 0.0;
+            const double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52);
+            const bool bad = !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
+            if (!__any_sync(SG_FULL, bad)) {
+                double tot = d;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                    tot = __dadd_rn(tot, __shfl_xor_sync(SG_FULL, tot, off));
+                const double M0 = __dmul_rn(P, iu);
+                if (tot <= __dsub_rn(M0, 0x1p52 + 1.0)) {
+                    P = __dmul_rn(__dsub_rn(M0, tot), sg_from_bits((uint64_t)(E - 52 + 1023) << 52));
+                    T = base + (uint32_t)nv;
+                    if (nv < 32)
+                        done = true;
+                    continue;
+                }
+            }
+        }
+
+        /* general case: advance P_notGuess over lanes [0, nv) in segments and
+         * take the codewords in order */
         int s = 0;
         while (s < nv && !done) {
             if (!(P >= 0x1p-970)) { /* zero, negative, tiny or NaN: one lane alone */
@@ -310,7 +343,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                 P = __dsub_rn(P, es);
                 if ((hits >> s) & 1u) {
                     const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
-                    if (sg_list_hit(ws, st, lp, hdm, mj, P, es, lane)) {
+                    if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
                         T = base + (uint32_t)s + 1u;
                         done = true;
                     }
@@ -345,7 +378,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                 const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
                 const double eh = __shfl_sync(SG_FULL, e, h);
                 const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
-                if (sg_list_hit(ws, st, lp, hdm, mj, Ph, eh, lane)) {
+                if (sg_list_hit(st, lp, hdm, mj, Ph, eh, lane, myrank)) {
                     T = base + (uint32_t)h + 1u;
                     done = true;
                     break;
@@ -361,7 +394,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                 P = __dsub_rn(P, es);
                 if ((hits >> f) & 1u) {
                     const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
-                    if (sg_list_hit(ws, st, lp, hdm, mj, P, es, lane)) {
+                    if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
                         T = base + (uint32_t)f + 1u;
                         done = true;
                     }
@@ -394,8 +427,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         pp0 = fmin(fmax(pp0, 1e-40), 1.0);
         double p1 = 0.0, p0 = 0.0;
         for (int j = 0; j < st.curl; j++) {
-            const double c = (double)((ws->cmask[j] >> lane) & 1u);
-            const double pj = ws->elist[j];
+            const double c = (double)((__shfl_sync(SG_FULL, st.my_cm, j) >> lane) & 1u);
+            const double pj = __shfl_sync(SG_FULL, st.my_e, j);
             p1 = __dadd_rn(p1, __dmul_rn(c, pj));
             p0 = __dadd_rn(p0, __dmul_rn(__dsub_rn(1.0, c), pj));
         }

@@ -119,6 +119,40 @@ SG_HD double sg_exp(double x, const double* tab)
     return e > 0 ? y * 0x1p64 : y * 0x1p-64;
 }
 
+/* exp(x) for x <= 0, bit-identical to sg_exp: the same operations without
+ * the range checks that cannot fire for arguments above -707.5 (the guess
+ * loop's exp(-PM), PM >= 0). */
+SG_HD double sg_exp_neg(double x, const double* tab)
+{
+    if (x < -707.5)
+        return sg_exp(x, tab);
+    double z = x * SG_EXP_INV_LN2_N;
+    double kd = z + SG_EXP_SHIFT;
+    int k = (int)(uint32_t)sg_bits(kd);
+    kd = kd - SG_EXP_SHIFT;
+    double r = sg_fma(-kd, SG_EXP_LN2_N_HI, x);
+    r = sg_fma(-kd, SG_EXP_LN2_N_LO, r);
+    int j = k & 127;
+    int e = k >> 7;
+#if defined(__CUDA_ARCH__)
+    const double2 Ht = reinterpret_cast<const double2*>(tab)[j];
+    const double H = Ht.x, t = Ht.y;
+#else
+    const double H = tab[2 * j], t = tab[2 * j + 1];
+#endif
+    double r2 = r * r;
+    double p = sg_fma(r, SG_EXP_C7, SG_EXP_C6);
+    p = sg_fma(r, p, SG_EXP_C5);
+    p = sg_fma(r, p, SG_EXP_C4);
+    p = sg_fma(r, p, SG_EXP_C3);
+    p = sg_fma(r, p, SG_EXP_C2);
+    p = p * r2;
+    double u = sg_fma(t, r, t);
+    double tmp = r + (u + p);
+    double S = sg_from_bits(sg_bits(H) + ((uint64_t)(int64_t)e << 52));
+    return sg_fma(S, tmp, S);
+}
+
 /* TwoSum: s + err == a + b exactly. */
 SG_HD double sg_two_sum(double a, double b, double* err)
 {
