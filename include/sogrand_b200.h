@@ -129,6 +129,33 @@ sg_status sg_bitso_host(const double* llr, size_t n_lines, int32_t L, uint64_t T
 sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_params* p,
                          size_t chunk_cw, sg_run_summary* summary);
 
+/* Totals of a device decode, with the comparator's bit and block errors
+ * (SOGRAND_C/comparator.c:31-60) when reference info bits are given. */
+typedef struct {
+    uint64_t blocks;          /* codewords decoded */
+    uint64_t converged;       /* codewords whose early termination fired */
+    uint64_t nonfinite;       /* codewords rejected for non-finite LLRs */
+    uint64_t total_ng;        /* sum of per-codeword NG */
+    uint64_t total_ng_p;      /* sum of per-codeword NG_p */
+    uint64_t bits_compared;   /* 512 per codeword when ref_info is given */
+    uint64_t bit_errors;      /* decoded info bits differing from ref_info */
+    uint64_t block_errors;    /* codewords with at least one bit error */
+    double total_iterations;  /* sum of per-codeword iterations (exact) */
+} sg_decode_summary;
+
+/* Decode and reduce on the device: bits (nullable: not returned) and one
+ * sg_decode_summary at d_summary (device memory, overwritten).  d_ref_info
+ * (nullable): the transmitted info bits, 64 packed bytes per codeword, for
+ * the bit and block error counts.  Per-codeword statistics are held in
+ * stream-ordered scratch (cudaMallocAsync) for the duration of the call. */
+sg_status sg_decode_summary_device(const double* d_llr, size_t n_cw, const sg_params* p,
+                                   const uint8_t* d_ref_info, uint8_t* d_bits,
+                                   sg_decode_summary* d_summary, void* stream);
+
+/* Wilson score interval for k successes in n trials at standard-normal
+ * quantile z (1.959963984540054 for 95%): *lo <= k/n <= *hi. */
+sg_status sg_wilson_interval(uint64_t k, uint64_t n, double z, double* lo, double* hi);
+
 /* ---- synthetic source, encoder and channel (pipeline stages before the
  * decoder: generate_bin.c, cubic_encoder.c, channel_sim.c).  The reference
  * seeds with time(NULL) and rand(); these are seeded and counter-based, so

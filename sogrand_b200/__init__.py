@@ -23,7 +23,7 @@ from ._lib import (SG_CUBE, SG_INFO_BYTES, SG_MAX_PHASES, SgCwStats, SgParams,
 
 __all__ = [
     "SG_CUBE", "SG_INFO_BYTES", "STATS_DTYPE", "SograndError", "params", "reference_alpha",
-    "decode", "bitso", "decode_file", "channel_sigma", "gen_info", "encode", "gen_llr",
+    "decode", "bitso", "decode_file", "decode_summary", "wilson_interval", "SUMMARY_DTYPE", "channel_sigma", "gen_info", "encode", "gen_llr",
     "version",
 ]
 
@@ -134,6 +134,35 @@ def decode_file(in_path: str, out_path: str, p: SgParams | None = None, chunk_cw
     s = SgRunSummary()
     check(_lib.load().sg_decode_file(in_path.encode(), out_path.encode(), C.byref(p), chunk_cw, C.byref(s)))
     return {k: getattr(s, k) for k, _ in SgRunSummary._fields_}
+
+
+SUMMARY_DTYPE = np.dtype([("blocks", "<u8"), ("converged", "<u8"), ("nonfinite", "<u8"), ("total_ng", "<u8"),
+                          ("total_ng_p", "<u8"), ("bits_compared", "<u8"), ("bit_errors", "<u8"),
+                          ("block_errors", "<u8"), ("total_iterations", "<f8")])
+
+
+def decode_summary(llr, p: SgParams | None = None, ref_info=None, want_bits: bool = False, stream=None):
+    """Decode CUDA-resident cubes and reduce on the device: returns
+    (summary dict, bits or None).  ref_info (CUDA uint8 [n, 64]) adds the
+    comparator's bit/block error counts."""
+    import torch
+
+    p = p or params()
+    n = llr.numel() // SG_CUBE
+    dev = llr.device
+    summ = torch.zeros(SUMMARY_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    bits = torch.empty((n, SG_INFO_BYTES), dtype=torch.uint8, device=dev) if want_bits else None
+    s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    check(_lib.load().sg_decode_summary_device(_ptr(llr), n, C.byref(p), _ptr(ref_info), _ptr(bits), _ptr(summ), s))
+    rec = np.frombuffer(summ.cpu().numpy().tobytes(), dtype=SUMMARY_DTYPE)[0]
+    return {k: rec[k].item() for k in SUMMARY_DTYPE.names}, bits
+
+
+def wilson_interval(k: int, n: int, conf_z: float = 1.959963984540054) -> tuple[float, float]:
+    """95% (default) Wilson score interval of the rate k/n."""
+    lo, hi = C.c_double(), C.c_double()
+    check(_lib.load().sg_wilson_interval(int(k), int(n), float(conf_z), C.byref(lo), C.byref(hi)))
+    return lo.value, hi.value
 
 
 def channel_sigma(ebn0_db: float) -> float:

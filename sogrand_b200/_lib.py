@@ -62,6 +62,20 @@ class SgRunSummary(C.Structure):
     ]
 
 
+class SgDecodeSummary(C.Structure):
+    _fields_ = [
+        ("blocks", C.c_uint64),
+        ("converged", C.c_uint64),
+        ("nonfinite", C.c_uint64),
+        ("total_ng", C.c_uint64),
+        ("total_ng_p", C.c_uint64),
+        ("bits_compared", C.c_uint64),
+        ("bit_errors", C.c_uint64),
+        ("block_errors", C.c_uint64),
+        ("total_iterations", C.c_double),
+    ]
+
+
 # every symbol include/sogrand_b200.h declares, with its signature
 _VP = C.c_void_p
 _SIGS = {
@@ -71,6 +85,9 @@ _SIGS = {
     "sg_bitso_device": (C.c_int, [_VP, C.c_size_t, C.c_int32, C.c_uint64, C.c_double, _VP, _VP, _VP, _VP, _VP]),
     "sg_bitso_host": (C.c_int, [_VP, C.c_size_t, C.c_int32, C.c_uint64, C.c_double, _VP, _VP, _VP, _VP]),
     "sg_decode_file": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(SgParams), C.c_size_t, C.POINTER(SgRunSummary)]),
+    "sg_decode_summary_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),
+    "sg_wilson_interval": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]),
     "sg_channel_sigma": (C.c_double, [C.c_double]),
     "sg_gen_info_host": (C.c_int, [C.c_uint64, C.c_uint64, C.c_size_t, _VP]),
     "sg_encode_host": (C.c_int, [_VP, C.c_size_t, _VP]),

@@ -392,6 +392,62 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
     }
 }
 
+/* Reduction of per-codeword statistics and bit errors into one
+ * sg_decode_summary (zeroed by the caller).  Iteration totals are sums of
+ * multiples of 0.5 below 2^52, so the atomic double additions are exact and
+ * the result does not depend on their order. */
+__global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __restrict__ stats,
+                                                          const uint8_t* __restrict__ bits,
+                                                          const uint8_t* __restrict__ ref,
+                                                          unsigned long long n, sg_decode_summary* out)
+{
+    unsigned long long conv = 0, nonf = 0, ng = 0, ngp = 0, be = 0, ble = 0;
+    double it = 0.0;
+    for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (unsigned long long)gridDim.x * blockDim.x) {
+        const sg_cw_stats st = stats[c];
+        conv += st.converged == 1;
+        nonf += st.converged < 0;
+        ng += st.ng;
+        ngp += st.ng_p;
+        it += st.iterations;
+        if (ref) {
+            const uint4* a = reinterpret_cast<const uint4*>(bits + c * SG_INFO_BYTES);
+            const uint4* b = reinterpret_cast<const uint4*>(ref + c * SG_INFO_BYTES);
+            unsigned int e = 0;
+            for (int q = 0; q < 4; q++) {
+                const uint4 x = a[q], y = b[q];
+                e += __popc(x.x ^ y.x) + __popc(x.y ^ y.y) + __popc(x.z ^ y.z) + __popc(x.w ^ y.w);
+            }
+            be += e;
+            ble += e != 0;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        conv += __shfl_xor_sync(SG_FULL, conv, off);
+        nonf += __shfl_xor_sync(SG_FULL, nonf, off);
+        ng += __shfl_xor_sync(SG_FULL, ng, off);
+        ngp += __shfl_xor_sync(SG_FULL, ngp, off);
+        be += __shfl_xor_sync(SG_FULL, be, off);
+        ble += __shfl_xor_sync(SG_FULL, ble, off);
+        it += __shfl_xor_sync(SG_FULL, it, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd((unsigned long long*)&out->converged, conv);
+        atomicAdd((unsigned long long*)&out->nonfinite, nonf);
+        atomicAdd((unsigned long long*)&out->total_ng, ng);
+        atomicAdd((unsigned long long*)&out->total_ng_p, ngp);
+        atomicAdd((unsigned long long*)&out->bit_errors, be);
+        atomicAdd((unsigned long long*)&out->block_errors, ble);
+        atomicAdd(&out->total_iterations, it);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd((unsigned long long*)&out->blocks, n);
+        if (ref)
+            atomicAdd((unsigned long long*)&out->bits_compared, n * (unsigned long long)SG_INFO_BITS);
+    }
+}
+
 /* Decoder kernel configurations: warps per codeword CTA, channel cube in
  * shared memory (bulk copy) or read from global memory, minimum resident
  * CTAs per SM for the register budget. */
@@ -444,7 +500,7 @@ struct DevCtx {
 };
 
 std::mutex g_mu;
-int g_variant = 0;
+int g_variant = 3; /* w16-gmem: fastest on B200 at 2 dB (sogrand_b200.autotune) */
 DevCtx g_ctx[64];
 std::vector<uint32_t> g_enum_host;
 sg_code_tables g_code;
@@ -860,6 +916,56 @@ size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
     const size_t m = n < cap ? n : cap;
     memcpy(out, t.data(), m * sizeof(uint32_t));
     return m;
+}
+
+sg_status sg_decode_summary_device(const double* d_llr, size_t n_cw, const sg_params* p,
+                                   const uint8_t* d_ref_info, uint8_t* d_bits, sg_decode_summary* d_summary,
+                                   void* stream)
+{
+    if (!d_summary)
+        return fail(SG_ERR_ARG, "summary must not be NULL");
+    if (d_ref_info && ((uintptr_t)d_ref_info & 15u))
+        return fail(SG_ERR_ARG, "ref_info must be 16-byte aligned");
+    if (d_bits && ((uintptr_t)d_bits & 15u))
+        return fail(SG_ERR_ARG, "bits must be 16-byte aligned");
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    SG_CUDA(cudaMemsetAsync(d_summary, 0, sizeof(sg_decode_summary), st));
+    if (n_cw == 0)
+        return SG_OK;
+    const size_t stat_bytes = ((n_cw * sizeof(sg_cw_stats) + 255) / 256) * 256;
+    const size_t bit_bytes = d_bits ? 0 : n_cw * SG_INFO_BYTES;
+    unsigned char* scratch = nullptr;
+    SG_CUDA(cudaMallocAsync((void**)&scratch, stat_bytes + bit_bytes, st));
+    sg_cw_stats* stats = reinterpret_cast<sg_cw_stats*>(scratch);
+    uint8_t* bits = d_bits ? d_bits : scratch + stat_bytes;
+    s = sg_decode_device(d_llr, n_cw, p, bits, nullptr, stats, stream);
+    if (s == SG_OK) {
+        sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw,
+                                                                                  d_summary);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            s = cuda_fail(e, "summary kernel");
+    }
+    cudaError_t e = cudaFreeAsync(scratch, st);
+    if (s == SG_OK && e != cudaSuccess)
+        s = cuda_fail(e, "cudaFreeAsync");
+    return s;
+}
+
+sg_status sg_wilson_interval(uint64_t k, uint64_t n, double z, double* lo, double* hi)
+{
+    if (!lo || !hi || n == 0 || k > n || !(z > 0))
+        return fail(SG_ERR_ARG, "wilson interval needs 0 <= k <= n, n > 0, z > 0");
+    const double nn = (double)n, ph = (double)k / nn, z2 = z * z;
+    const double den = 1.0 + z2 / nn;
+    const double c = (ph + z2 / (2 * nn)) / den;
+    const double h = z * sqrt(ph * (1 - ph) / nn + z2 / (4 * nn * nn)) / den;
+    *lo = (k == 0 || c - h < 0) ? 0.0 : c - h;
+    *hi = (k == n || c + h > 1) ? 1.0 : c + h;
+    return SG_OK;
 }
 
 int sg_decoder_variant_count(void) { return SG_NVARIANTS; }

@@ -94,3 +94,13 @@ def test_cli_usage(sg):
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 1
     assert r.stderr.startswith("Usage: ") and "<input_llr_file> <output_file>" in r.stderr
+
+
+def test_wilson_interval(sg):
+    lo, hi = sg.wilson_interval(0, 1000)
+    assert lo == 0.0 and 0.0038 < hi < 0.0039
+    lo, hi = sg.wilson_interval(50, 100)
+    assert abs(lo - 0.40383) < 1e-4 and abs(hi - 0.59617) < 1e-4
+    assert sg.wilson_interval(7, 7)[1] == 1.0
+    with pytest.raises(sg.SograndError):
+        sg.wilson_interval(5, 4)
