@@ -228,8 +228,10 @@ def main():
     elif args.autotune:
         tune = autotune.autotune(device=local)
     # every rank decodes its own codeword range of the same stream (no data-path collective)
+    from sogrand_b200.replicas import codeword_range, max_over_ranks
+
     n = args.n_cw
-    cw0 = rank * n
+    cw0, _ = codeword_range(rank, world, n_per_rank=n)
     stream = torch.cuda.Stream(dev)
     p = sg.params()
     lib = _lib.load()
@@ -259,11 +261,7 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     dt = ev0.elapsed_time(ev1) / 1000.0
-    t_max = dt
-    if pg:
-        t = torch.tensor([dt], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(dt, device=dev) if pg else dt
     value = world * n * args.steps / t_max
 
     # results of the timed run (one step's worth) for the sanity fields
@@ -290,9 +288,7 @@ def main():
                                           stats_h.ctypes.data))
         e2e_dt = (time.perf_counter() - t0) / args.e2e_steps
         if pg:
-            t = torch.tensor([e2e_dt], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_dt = float(t.item())
+            e2e_dt = max_over_ranks(e2e_dt, device=dev)
         e2e = {"value": world * n / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": n * 4096 * 8,
                "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
                "api": "sg_decode_host (host buffers, copies inside the timed region)"}
