@@ -152,6 +152,31 @@ sg_status sg_decode_summary_device(const double* d_llr, size_t n_cw, const sg_pa
                                    const uint8_t* d_ref_info, uint8_t* d_bits,
                                    sg_decode_summary* d_summary, void* stream);
 
+/* ---- allocation-free variant of sg_decode_summary_device.
+ *
+ * For callers that must not allocate device memory at all: code that runs
+ * while another component owns the device allocator (a framework's caching
+ * pool, a real-time process that forbids allocation after start-up), or
+ * code whose every device buffer is budgeted up front.  The regular entry
+ * point takes stream-ordered scratch per call and its first call on a device
+ * allocates the 15 MB error-pattern order table; this one uses only memory
+ * that the library declares statically:
+ *   - scratch for at most SG_NOALLOC_MAX_CW codewords (statistics and bits,
+ *     1.5 MB in all), held by every GPU that loads the library until exit;
+ *   - its own copy of the pattern-order table (15 MB, also static), built on
+ *     the device by a kernel during the first call on each device.
+ * That first call also resolves the device addresses of these arrays and
+ * sets up the device; make it before any stream capture.  n_cw above
+ * SG_NOALLOC_MAX_CW is rejected with SG_ERR_ARG.  All calls share the one
+ * scratch array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Results equal those
+ * of sg_decode_summary_device.  This entry point has no counterpart in the
+ * reference, which is a single-process file pipeline. */
+#define SG_NOALLOC_MAX_CW 16384
+sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, const sg_params* p,
+                                           const uint8_t* d_ref_info, uint8_t* d_bits,
+                                           sg_decode_summary* d_summary, void* stream);
+
 /* Wilson score interval for k successes in n trials at standard-normal
  * quantile z (1.959963984540054 for 95%): *lo <= k/n <= *hi. */
 sg_status sg_wilson_interval(uint64_t k, uint64_t n, double z, double* lo, double* hi);

@@ -86,6 +86,7 @@ _SIGS = {
     "sg_bitso_host": (C.c_int, [_VP, C.c_size_t, C.c_int32, C.c_uint64, C.c_double, _VP, _VP, _VP, _VP]),
     "sg_decode_file": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(SgParams), C.c_size_t, C.POINTER(SgRunSummary)]),
     "sg_decode_summary_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),
+    "sg_decode_summary_device_noalloc": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),
     "sg_wilson_interval": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double)]),
     "sg_channel_sigma": (C.c_double, [C.c_double]),

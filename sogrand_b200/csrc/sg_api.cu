@@ -469,6 +469,26 @@ static const SgVariant g_variants[] = {
 };
 #define SG_NVARIANTS ((int)(sizeof(g_variants) / sizeof(g_variants[0])))
 
+/* Static device memory of the allocation-free entry point: the error flag
+ * (first 256 bytes), then per-codeword statistics and bits for at most
+ * SG_NOALLOC_MAX_CW codewords; and a private copy of the pattern-order
+ * tables.  Host code must not use these names as addresses: the set-up
+ * below resolves them with cudaGetSymbolAddress on each device. */
+#define SG_NOALLOC_HDR 256
+#define SG_NOALLOC_STATS_BYTES (SG_NOALLOC_MAX_CW * sizeof(sg_cw_stats))
+#define SG_NOALLOC_BYTES (SG_NOALLOC_HDR + SG_NOALLOC_STATS_BYTES + SG_NOALLOC_MAX_CW * SG_INFO_BYTES)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SG_NOALLOC_BYTES];
+static __device__ __align__(256) uint32_t g_noalloc_enum[SG_ENUM_NTAB * SG_ENUM_LEN];
+
+/* One thread per IC builds that IC's pattern order (same source as the host
+ * builder); ok[ic] = 1 when complete. */
+__global__ void sg_enum_build_kernel(uint32_t* out, unsigned int* ok)
+{
+    const int ic = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ic < SG_ENUM_NTAB)
+        ok[ic] = sg_enum_build_impl(ic, out + (size_t)ic * SG_ENUM_LEN) == SG_ENUM_LEN ? 1u : 0u;
+}
+
 /* -------------------------------------------------------------- host -- */
 
 namespace {
@@ -965,6 +985,111 @@ sg_status sg_wilson_interval(uint64_t k, uint64_t n, double z, double* lo, doubl
     const double h = z * sqrt(ph * (1 - ph) / nn + z2 / (4 * nn * nn)) / den;
     *lo = (k == 0 || c - h < 0) ? 0.0 : c - h;
     *hi = (k == n || c + h > 1) ? 1.0 : c + h;
+    return SG_OK;
+}
+
+namespace {
+
+struct NoAllocCtx {
+    bool ready = false;
+    unsigned char* scratch = nullptr; /* device address of g_noalloc_scratch */
+    uint32_t* enum_tabs = nullptr;    /* device address of g_noalloc_enum */
+};
+NoAllocCtx g_noalloc[64];
+
+/* Once per device, with that device current: resolve the static arrays'
+ * device addresses, load the code tables, build the pattern orders on the
+ * device, allow the decode kernels their shared memory.  No allocation. */
+sg_status noalloc_setup(NoAllocCtx** out)
+{
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64)
+        return fail(SG_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    NoAllocCtx& c = g_noalloc[dev];
+    if (!c.ready) {
+        sg_code_tables code;
+        sg_code_build(&code);
+        SG_CUDA(cudaGetSymbolAddress((void**)&c.scratch, g_noalloc_scratch));
+        SG_CUDA(cudaGetSymbolAddress((void**)&c.enum_tabs, g_noalloc_enum));
+        SG_CUDA(cudaMemcpyToSymbol(c_hcol, code.hcol, sizeof code.hcol));
+        SG_CUDA(cudaMemcpyToSymbol(c_prow, code.prow, sizeof code.prow));
+        SG_CUDA(cudaMemcpyToSymbol(c_ptab, code.ptab, sizeof code.ptab));
+        for (int v = 0; v < SG_NVARIANTS; v++)
+            SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_variants[v].smem));
+        /* the completion flags of the build borrow the scratch array */
+        unsigned int* ok = reinterpret_cast<unsigned int*>(c.scratch);
+        SG_CUDA(cudaMemset(ok, 0, SG_ENUM_NTAB * sizeof(unsigned int)));
+        sg_enum_build_kernel<<<1, 64>>>(c.enum_tabs, ok);
+        SG_CUDA(cudaGetLastError());
+        unsigned int hok[SG_ENUM_NTAB];
+        SG_CUDA(cudaMemcpy(hok, ok, sizeof hok, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < SG_ENUM_NTAB; i++)
+            if (hok[i] != 1u)
+                return fail(SG_ERR_ARG, "device pattern-order build incomplete");
+        c.ready = true;
+    }
+    *out = &c;
+    return SG_OK;
+}
+
+} // namespace
+
+sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, const sg_params* p,
+                                           const uint8_t* d_ref_info, uint8_t* d_bits,
+                                           sg_decode_summary* d_summary, void* stream)
+{
+    if (!d_summary)
+        return fail(SG_ERR_ARG, "summary must not be NULL");
+    if (n_cw > SG_NOALLOC_MAX_CW)
+        return fail(SG_ERR_ARG, "n_cw exceeds SG_NOALLOC_MAX_CW (16384) for the allocation-free entry point");
+    if (d_ref_info && ((uintptr_t)d_ref_info & 15u))
+        return fail(SG_ERR_ARG, "ref_info must be 16-byte aligned");
+    if (d_bits && ((uintptr_t)d_bits & 15u))
+        return fail(SG_ERR_ARG, "bits must be 16-byte aligned");
+    if (n_cw && !d_llr)
+        return fail(SG_ERR_ARG, "llr must not be NULL");
+    if ((uintptr_t)d_llr & 7u)
+        return fail(SG_ERR_ARG, "llr must be 8-byte aligned");
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    NoAllocCtx* c = nullptr;
+    if ((s = noalloc_setup(&c)) != SG_OK)
+        return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    SG_CUDA(cudaMemsetAsync(d_summary, 0, sizeof(sg_decode_summary), st));
+    if (n_cw == 0)
+        return SG_OK;
+    /* the scratch keeps the previous call's contents: clear the error flag;
+     * statistics and bits are overwritten for every codeword */
+    unsigned int* err = reinterpret_cast<unsigned int*>(c->scratch);
+    sg_cw_stats* stats = reinterpret_cast<sg_cw_stats*>(c->scratch + SG_NOALLOC_HDR);
+    uint8_t* bits = d_bits ? d_bits : c->scratch + SG_NOALLOC_HDR + SG_NOALLOC_STATS_BYTES;
+    SG_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned int), st));
+    SgDecodeArgs a;
+    memset(&a, 0, sizeof a);
+    a.llr = d_llr;
+    a.bits = bits;
+    a.lapp = nullptr;
+    a.stats = stats;
+    a.enum_tabs = c->enum_tabs;
+    a.err = err;
+    a.n_cw = n_cw;
+    a.L = p->L;
+    a.imax = p->Imax;
+    a.tmax = tmax_eff(p->Tmax);
+    a.use_bulk = ((uintptr_t)d_llr & 15u) == 0;
+    a.thres = p->thres;
+    memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    const SgVariant& v = g_variants[g_variant];
+    void* kargs[] = {(void*)&a};
+    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid_for(n_cw, 1 << 30)), dim3(v.nw * 32), kargs, v.smem, st));
+    sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw,
+                                                                              d_summary);
+    SG_CUDA(cudaGetLastError());
     return SG_OK;
 }
 
