@@ -193,6 +193,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cw-per-core", type=int, default=16)
     ap.add_argument("--ref-cw-per-core", type=int, default=4)
+    ap.add_argument("--form", default="batch", choices=["plain", "batch"],
+                    help="plain: one CTA per codeword (sg_decode_device); batch: persistent kernel replayed "
+                         "from a CUDA graph (sg_batch_*)")
+    ap.add_argument("--workload", default="2dB", choices=["2dB", "mixed"],
+                    help="2dB: Eb/N0 2.0 dB; mixed: per-codeword Eb/N0 uniform in [1, 3] dB")
     ap.add_argument("--variant", default=None, help="decoder kernel variant (name or index)")
     ap.add_argument("--autotune", action="store_true", help="measure all variants first, keep the fastest")
     ap.add_argument("--port-worker", default=None, help=argparse.SUPPRESS)
@@ -222,11 +227,15 @@ def main():
         pg = dist
     from sogrand_b200 import autotune
 
+    from sogrand_b200 import batch as B
+
     tune = None
+    snr_kw = dict(ebn0_db=EBN0) if args.workload == "2dB" else dict(ebn0_range=(1.0, 3.0))
     if args.variant is not None:
-        autotune.set_variant(int(args.variant) if args.variant.isdigit() else args.variant)
+        setv = B.set_variant if args.form == "batch" else autotune.set_variant
+        setv(int(args.variant) if args.variant.isdigit() else args.variant)
     elif args.autotune:
-        tune = autotune.autotune(device=local)
+        tune = (autotune.autotune_batch if args.form == "batch" else autotune.autotune)(device=local, **snr_kw)
     # every rank decodes its own codeword range of the same stream (no data-path collective)
     from sogrand_b200.replicas import codeword_range, max_over_ranks
 
@@ -236,14 +245,21 @@ def main():
     p = sg.params()
     lib = _lib.load()
     with torch.cuda.stream(stream):
-        info, llr = sg.gen_llr(SEED, cw0, n, ebn0_db=EBN0, device=dev, stream=stream.cuda_stream)
+        info, llr = sg.gen_llr(SEED, cw0, n, device=dev, stream=stream.cuda_stream, **snr_kw)
         bits = torch.empty((n, 64), dtype=torch.uint8, device=dev)
         stats = torch.empty((n, sg.STATS_DTYPE.itemsize), dtype=torch.uint8, device=dev)
     stream.synchronize()
+    batch = None
+    if args.form == "batch":
+        batch = B.Batch()
+        batch.capture(llr, bits, stats, p, stream=stream.cuda_stream)
 
     def decode_step():
-        _lib.check(lib.sg_decode_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), None, stats.data_ptr(),
-                                        stream.cuda_stream))
+        if batch is not None:
+            batch.replay(stream.cuda_stream)
+        else:
+            _lib.check(lib.sg_decode_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), None,
+                                            stats.data_ptr(), stream.cuda_stream))
 
     for _ in range(args.warmup):
         decode_step()
@@ -306,16 +322,19 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"cubic (16,8)^3 SOGRAND decode, {n} codewords per GPU per step, "
-                                   f"Eb/N0 {EBN0} dB, L=3 Imax=30 Tmax=inf",
-                       "codewords_per_gpu": n, "ebn0_db": EBN0, "parallelism": f"replicas{world}",
-                       "l2": "inputs (3.3 GB per GPU) larger than L2; no flush"},
+                                   + (f"Eb/N0 {EBN0} dB" if args.workload == "2dB" else "Eb/N0 U[1,3] dB per codeword")
+                                   + ", L=3 Imax=30 Tmax=inf",
+                       "codewords_per_gpu": n, "ebn0_db": EBN0 if args.workload == "2dB" else [1.0, 3.0],
+                       "form": args.form, "parallelism": f"replicas{world}",
+                       "l2": f"inputs ({n * 32768 / 1e9:.1f} GB per GPU) larger than L2; no flush"},
             "info_mbps": value * 512 / 1e6,
             "ber": ber, "ng_per_codeword": ng_per_cw, "guesses_per_s": value * ng_per_cw,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": None,
                          "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},
             "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
-            "variant": autotune.get_variant(), "autotune": tune,
+            "form": args.form, "autotune": tune,
+            "variant": B.get_variant() if args.form == "batch" else autotune.get_variant(),
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)

@@ -209,6 +209,33 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
                             double ebn0_lo_db, double ebn0_hi_db, uint8_t* d_info,
                             double* d_llr, void* stream);
 
+/* ---- batched persistent decoder.  One resident CTA per SM holds several
+ * codeword slots; warps take lines from any slot with work, the warp that
+ * completes a phase runs early termination and either opens the slot's next
+ * phase or retires the codeword and admits the next one from a device work
+ * queue.  No CTA-wide barrier, so codewords of very uneven cost (mixed
+ * Eb/N0) do not stall each other.  Outputs are bit-identical to
+ * sg_decode_device.  A handle owns the work-queue word (device memory
+ * allocated by sg_batch_create on the current device) and an optional CUDA
+ * graph of one decode. */
+typedef struct sg_batch_s* sg_batch;
+sg_status sg_batch_create(sg_batch* out);
+sg_status sg_batch_destroy(sg_batch b);
+/* Enqueue one batched decode on `stream` (capturable; one in flight per handle). */
+sg_status sg_batch_decode(sg_batch b, const double* d_llr, size_t n_cw, const sg_params* p,
+                          uint8_t* d_bits, double* d_lapp, sg_cw_stats* d_stats, void* stream);
+/* Record the same decode (queue reset + kernel) as a CUDA graph held by the
+ * handle; sg_batch_replay launches it again on any stream. */
+sg_status sg_batch_capture(sg_batch b, const double* d_llr, size_t n_cw, const sg_params* p,
+                           uint8_t* d_bits, double* d_lapp, sg_cw_stats* d_stats, void* stream);
+sg_status sg_batch_replay(sg_batch b, void* stream);
+/* After the decode completed: SG_ERR_TIMEOUT if a bounded wait gave up. */
+sg_status sg_batch_check(sg_batch b);
+int sg_batch_variant_count(void);
+const char* sg_batch_variant_name(int v);
+sg_status sg_batch_set_variant(int v);
+int sg_batch_get_variant(void);
+
 /* ---- kernel configuration (process-wide).  Variants differ in warps per
  * codeword CTA and in where the 32 KB channel cube is held (shared memory,
  * staged by a bulk asynchronous copy, or global memory through L2); all give

@@ -98,6 +98,16 @@ _SIGS = {
         [C.c_uint64, C.c_uint64, C.c_size_t, C.c_double, C.c_double, C.c_double, _VP, _VP, _VP],
     ),
     "sg_pattern_order": (C.c_size_t, [C.c_int32, _VP, C.c_size_t]),
+    "sg_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "sg_batch_destroy": (C.c_int, [_VP]),
+    "sg_batch_decode": (C.c_int, [_VP, _VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),
+    "sg_batch_capture": (C.c_int, [_VP, _VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),
+    "sg_batch_replay": (C.c_int, [_VP, _VP]),
+    "sg_batch_check": (C.c_int, [_VP]),
+    "sg_batch_variant_count": (C.c_int, []),
+    "sg_batch_variant_name": (C.c_char_p, [C.c_int]),
+    "sg_batch_set_variant": (C.c_int, [C.c_int]),
+    "sg_batch_get_variant": (C.c_int, []),
     "sg_decoder_variant_count": (C.c_int, []),
     "sg_decoder_variant_name": (C.c_char_p, [C.c_int]),
     "sg_decoder_set_variant": (C.c_int, [C.c_int]),

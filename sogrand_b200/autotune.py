@@ -29,7 +29,7 @@ def get_variant() -> str:
     return lib.sg_decoder_variant_name(lib.sg_decoder_get_variant()).decode()
 
 
-def autotune(n_cw: int = 148 * 3 * 20, ebn0_db: float | None = 2.0, ebn0_range=None, seed: int = 1,
+def autotune(n_cw: int = 148 * 3 * 20, ebn0_db: float | None = None, ebn0_range=None, seed: int = 1,
              device: int = 0, params=None, repeats: int = 1) -> dict:
     """Measure every variant on n_cw synthetic codewords; select the fastest.
     Returns {variant name: codewords/s} plus "best"."""
@@ -40,6 +40,8 @@ def autotune(n_cw: int = 148 * 3 * 20, ebn0_db: float | None = 2.0, ebn0_range=N
     lib = _lib.load()
     dev = torch.device("cuda", device)
     p = params or sg.params()
+    if ebn0_db is None and ebn0_range is None:
+        ebn0_db = 2.0
     _, llr = sg.gen_llr(seed, 0, n_cw, ebn0_db=ebn0_db, ebn0_range=ebn0_range, device=dev)
     bits = torch.empty((n_cw, sg.SG_INFO_BYTES), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -58,5 +60,38 @@ def autotune(n_cw: int = 148 * 3 * 20, ebn0_db: float | None = 2.0, ebn0_range=N
         res[name] = repeats * n_cw / (e0.elapsed_time(e1) / 1000.0)
     best = max(res, key=res.get)
     set_variant(best)
+    res["best"] = best
+    return res
+
+
+def autotune_batch(n_cw: int = 148 * 3 * 20, ebn0_db: float | None = None, ebn0_range=None, seed: int = 1,
+                   device: int = 0, params=None) -> dict:
+    """Measure every batched (persistent) variant; select the fastest."""
+    import torch
+
+    import sogrand_b200 as sg
+    from . import batch as B
+
+    lib = _lib.load()
+    dev = torch.device("cuda", device)
+    if ebn0_db is None and ebn0_range is None:
+        ebn0_db = 2.0
+    _, llr = sg.gen_llr(seed, 0, n_cw, ebn0_db=ebn0_db, ebn0_range=ebn0_range, device=dev)
+    b = B.Batch()
+    res = {}
+    for v, name in enumerate(B.variants()):
+        _lib.check(lib.sg_batch_set_variant(v))
+        b.decode(llr, params)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.current_stream(dev)
+        e0.record(stream)
+        b.decode(llr, params)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        b.check()
+        res[name] = n_cw / (e0.elapsed_time(e1) / 1000.0)
+    best = max(res, key=res.get)
+    B.set_variant(best)
+    b.close()
     res["best"] = best
     return res

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <errno.h>
+#include <stddef.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +27,7 @@
 
 #include <chrono>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -66,10 +68,10 @@ struct SgDecodeArgs {
  * global memory (L2-resident) once per phase. */
 template <int NW, bool LCH_SMEM>
 struct SgCwSmem {
-    double lch[LCH_SMEM ? SG_CUBE : 2];
+    alignas(16) double lch[LCH_SMEM ? SG_CUBE : 2]; /* bulk-copy destination */
     double le[SG_CUBE];
-    double etab[SG_EXP_TAB_LEN];
-    double ltab[SG_LOG_TAB_LEN];
+    alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by sg_exp_neg */
+    alignas(16) double ltab[SG_LOG_TAB_LEN];
     SgWarpScratch ws[NW];
     uint16_t hdw[256];
     unsigned long long mbar;
@@ -132,7 +134,7 @@ __device__ __forceinline__ uint32_t sg_smem_u32(const void* p)
 
 extern __shared__ __align__(128) unsigned char sg_smem_raw[];
 
-template <int NW, bool LCH_SMEM, int MINB>
+template <int NW, bool LCH_SMEM, int MINB, int G>
 __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
 {
     constexpr int NT = NW * 32;
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
                     if (lane < 16) /* L_ch + (alpha*L_E) */
                         v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, S.le[pos]));
                     const SgLineResult r =
-                        sg_decode_line(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+                        sg_decode_line<G>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
                     if (lane < 16) {
                         S.le[pos] = r.le;
                         if (args.lapp)
@@ -303,9 +305,11 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
     }
 }
 
+#include "sg_persist.cuh"
+
 struct SgLineSmem {
-    double etab[SG_EXP_TAB_LEN];
-    double ltab[SG_LOG_TAB_LEN];
+    alignas(16) double etab[SG_EXP_TAB_LEN];
+    alignas(16) double ltab[SG_LOG_TAB_LEN];
     SgWarpScratch ws[SG_WARPS];
 };
 
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(SG_THREADS) sg_bitso_kernel(const double* __re
             }
             continue;
         }
-        const SgLineResult r = sg_decode_line(v, lp, enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+        const SgLineResult r = sg_decode_line<1>(v, lp, enum_tabs, S.etab, S.ltab, &S.ws[warp]);
         if (lane < 16) {
             lapp[l * 16 + lane] = r.lapp;
             le[l * 16 + lane] = r.le;
@@ -355,8 +359,8 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
                                                              double lo, double hi, uint8_t* info,
                                                              double* llr)
 {
-    __shared__ double etab[SG_EXP_TAB_LEN];
-    __shared__ double ltab[SG_LOG_TAB_LEN];
+    __shared__ alignas(16) double etab[SG_EXP_TAB_LEN];
+    __shared__ alignas(16) double ltab[SG_LOG_TAB_LEN];
     __shared__ uint16_t W[256];
     __shared__ uint8_t ib[SG_INFO_BYTES];
     __shared__ uint8_t prow[8];
@@ -459,15 +463,58 @@ struct SgVariant {
     const void* fn;
 };
 
-#define SG_VARIANT(NW, L, M, NAME) \
-    { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M> }
+#define SG_VARIANT(NW, L, M, G, NAME) \
+    { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M, G> }
 static const SgVariant g_variants[] = {
-    SG_VARIANT(8, false, 3, "w8-gmem"),
-    SG_VARIANT(8, true, 2, "w8-smem"),
-    SG_VARIANT(12, true, 2, "w12-smem"),
-    SG_VARIANT(16, false, 2, "w16-gmem"),
+    SG_VARIANT(8, false, 3, 1, "w8-gmem"),
+    SG_VARIANT(8, true, 2, 1, "w8-smem"),
+    SG_VARIANT(12, true, 2, 1, "w12-smem"),
+    SG_VARIANT(16, false, 2, 1, "w16-gmem"),
+    SG_VARIANT(16, false, 2, 2, "w16-gmem-g2"),
+    SG_VARIANT(8, false, 3, 2, "w8-gmem-g2"),
+    SG_VARIANT(12, true, 2, 2, "w12-smem-g2"),
 };
 #define SG_NVARIANTS ((int)(sizeof(g_variants) / sizeof(g_variants[0])))
+
+/* Batched persistent decoder configurations: warps per CTA (one CTA per
+ * SM), codeword slots per CTA. */
+struct SgPVariant {
+    const char* name;
+    int nw;
+    int slots;
+    size_t smem;
+    const void* fn;
+};
+#define SG_PVARIANT(NW, C, G, NAME) \
+    { NAME, NW, C, sizeof(SgPersistSmem<NW, C>), (const void*)sg_persist_kernel<NW, C, G> }
+static const SgPVariant g_pvariants[] = {
+    SG_PVARIANT(24, 3, 1, "p24x3"),
+    SG_PVARIANT(28, 4, 1, "p28x4"),
+    SG_PVARIANT(16, 3, 1, "p16x3"),
+    SG_PVARIANT(20, 4, 1, "p20x4"),
+    SG_PVARIANT(32, 3, 1, "p32x3"),
+};
+#define SG_NPVARIANTS ((int)(sizeof(g_pvariants) / sizeof(g_pvariants[0])))
+
+/* 16-byte alignment of the shared tables (double2 loads) and of the bulk
+ * copy destination, for every configuration built. */
+template <class T>
+constexpr bool sg_tables_aligned()
+{
+    return offsetof(T, etab) % 16 == 0 && offsetof(T, ltab) % 16 == 0;
+}
+static_assert(sg_tables_aligned<SgPersistSmem<24, 3>>() && sg_tables_aligned<SgPersistSmem<28, 4>>() &&
+                  sg_tables_aligned<SgPersistSmem<16, 3>>() && sg_tables_aligned<SgPersistSmem<20, 4>>() && sg_tables_aligned<SgPersistSmem<32, 3>>() &&
+                  sg_tables_aligned<SgCwSmem<8, false>>() && sg_tables_aligned<SgCwSmem<8, true>>() &&
+                  sg_tables_aligned<SgCwSmem<12, true>>() && sg_tables_aligned<SgCwSmem<16, false>>() &&
+                  sg_tables_aligned<SgLineSmem>(),
+              "shared table alignment");
+template <class T>
+constexpr bool sg_bulk_aligned()
+{
+    return offsetof(T, lch) == 0 && offsetof(T, mbar) % 8 == 0;
+}
+static_assert(sg_bulk_aligned<SgCwSmem<8, true>>() && sg_bulk_aligned<SgCwSmem<12, true>>(), "bulk copy");
 
 /* Static device memory of the allocation-free entry point: the error flag
  * (first 256 bytes), then per-codeword statistics and bits for at most
@@ -517,9 +564,11 @@ struct DevCtx {
     bool ready = false;
     uint32_t* enum_tabs = nullptr;
     unsigned int* err = nullptr;
+    int sms = 0;
 };
 
 std::mutex g_mu;
+int g_pvariant = 4; /* p32x3: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
 int g_variant = 3; /* w16-gmem: fastest on B200 at 2 dB (sogrand_b200.autotune) */
 DevCtx g_ctx[64];
 std::vector<uint32_t> g_enum_host;
@@ -565,6 +614,10 @@ sg_status get_ctx(DevCtx** out)
         for (int v = 0; v < SG_NVARIANTS; v++)
             SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)g_variants[v].smem));
+        for (int v = 0; v < SG_NPVARIANTS; v++)
+            SG_CUDA(cudaFuncSetAttribute(g_pvariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_pvariants[v].smem));
+        SG_CUDA(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
         c.ready = true;
     }
     *out = &c;
@@ -1092,6 +1145,175 @@ sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, con
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }
+
+} // extern "C"
+
+struct sg_batch_s {
+    int device = -1;
+    SgQueue* q = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+sg_status batch_enqueue(sg_batch b, const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
+                        double* d_lapp, sg_cw_stats* d_stats, cudaStream_t st)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (!b || !b->q)
+        return fail(SG_ERR_ARG, "invalid batch handle");
+    if (n_cw && (!d_llr || !d_bits))
+        return fail(SG_ERR_ARG, "llr and bits must not be NULL");
+    if ((uintptr_t)d_llr & 7u)
+        return fail(SG_ERR_ARG, "llr must be 8-byte aligned");
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    if (dev != b->device)
+        return fail(SG_ERR_ARG, "batch handle belongs to another device");
+    DevCtx* c = nullptr;
+    if ((s = get_ctx(&c)) != SG_OK)
+        return s;
+    SG_CUDA(cudaMemsetAsync(b->q, 0, sizeof(SgQueue), st));
+    if (n_cw == 0)
+        return SG_OK;
+    SgDecodeArgs a;
+    memset(&a, 0, sizeof a);
+    a.llr = d_llr;
+    a.bits = d_bits;
+    a.lapp = d_lapp;
+    a.stats = d_stats;
+    a.enum_tabs = c->enum_tabs;
+    a.err = c->err;
+    a.n_cw = n_cw;
+    a.L = p->L;
+    a.imax = p->Imax;
+    a.tmax = tmax_eff(p->Tmax);
+    a.use_bulk = 0;
+    a.thres = p->thres;
+    memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    const SgPVariant& v = g_pvariants[g_pvariant];
+    SgQueue* q = b->q;
+    void* kargs[] = {(void*)&a, (void*)&q};
+    const int grid = (int)(n_cw < (size_t)c->sms ? n_cw : (size_t)c->sms);
+    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem, st));
+    return SG_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+sg_status sg_batch_create(sg_batch* out)
+{
+    if (!out)
+        return fail(SG_ERR_ARG, "NULL handle pointer");
+    *out = nullptr;
+    DevCtx* c = nullptr;
+    sg_status s = get_ctx(&c);
+    if (s != SG_OK)
+        return s;
+    sg_batch b = new (std::nothrow) sg_batch_s;
+    if (!b)
+        return fail(SG_ERR_NOMEM, "host allocation failed");
+    cudaGetDevice(&b->device);
+    cudaError_t e = cudaMalloc(&b->q, sizeof(SgQueue));
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    *out = b;
+    return SG_OK;
+}
+
+sg_status sg_batch_destroy(sg_batch b)
+{
+    if (!b)
+        return SG_OK;
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    cudaFree(b->q);
+    delete b;
+    return SG_OK;
+}
+
+sg_status sg_batch_decode(sg_batch b, const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
+                          double* d_lapp, sg_cw_stats* d_stats, void* stream)
+{
+    return batch_enqueue(b, d_llr, n_cw, p, d_bits, d_lapp, d_stats, (cudaStream_t)stream);
+}
+
+sg_status sg_batch_capture(sg_batch b, const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
+                           double* d_lapp, sg_cw_stats* d_stats, void* stream)
+{
+    if (!b)
+        return fail(SG_ERR_ARG, "invalid batch handle");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStream_t own = nullptr;
+    if (!st) {
+        SG_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+        st = own;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    sg_status s = SG_OK;
+    if (e != cudaSuccess) {
+        s = cuda_fail(e, "cudaStreamBeginCapture");
+    } else {
+        s = batch_enqueue(b, d_llr, n_cw, p, d_bits, d_lapp, d_stats, st);
+        e = cudaStreamEndCapture(st, &g);
+        if (s == SG_OK && e != cudaSuccess)
+            s = cuda_fail(e, "cudaStreamEndCapture");
+    }
+    if (s == SG_OK) {
+        if (b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        e = cudaGraphInstantiate(&b->exec, g, 0);
+        if (e != cudaSuccess)
+            s = cuda_fail(e, "cudaGraphInstantiate");
+    }
+    if (g)
+        cudaGraphDestroy(g);
+    if (own)
+        cudaStreamDestroy(own);
+    return s;
+}
+
+sg_status sg_batch_replay(sg_batch b, void* stream)
+{
+    if (!b || !b->exec)
+        return fail(SG_ERR_ARG, "no captured decode in this batch handle");
+    SG_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+    return SG_OK;
+}
+
+sg_status sg_batch_check(sg_batch b)
+{
+    if (!b)
+        return fail(SG_ERR_ARG, "invalid batch handle");
+    SgQueue hq;
+    SG_CUDA(cudaMemcpy(&hq, b->q, sizeof hq, cudaMemcpyDeviceToHost));
+    if (hq.err)
+        return fail(SG_ERR_TIMEOUT, "a persistent-decoder warp gave up waiting for work");
+    return SG_OK;
+}
+
+int sg_batch_variant_count(void) { return SG_NPVARIANTS; }
+
+const char* sg_batch_variant_name(int v) { return (v >= 0 && v < SG_NPVARIANTS) ? g_pvariants[v].name : ""; }
+
+sg_status sg_batch_set_variant(int v)
+{
+    if (v < 0 || v >= SG_NPVARIANTS)
+        return fail(SG_ERR_ARG, "no such batch variant");
+    g_pvariant = v;
+    return SG_OK;
+}
+
+int sg_batch_get_variant(void) { return g_pvariant; }
 
 int sg_decoder_variant_count(void) { return SG_NVARIANTS; }
 

@@ -17,7 +17,7 @@
  *             synlo/hi  syndrome of each byte of a pattern (ParityCheck,
  *                       :748-755, is linear), the hard decision's own
  *                       syndrome folded into synlo.
- *  guesses  32 consecutive patterns of the order table per step, one per
+ *  guesses  32*G consecutive patterns of the order table per step, G per
  *           lane: PM = A[lo] + increments of the high bits (ascending),
  *           syndrome = synlo[lo] ^ synhi[hi], e = exp(-PM).
  *  P_notGuess  the reference subtracts e of every guess in order (:626,
@@ -25,10 +25,13 @@
  *           rounds to the grid u = 2^(E-52), so fl(P - e) = u*round(M - e/u)
  *           with M = P/u an integer: the running value is an exact integer
  *           prefix sum, computed by a warp scan (sums < 2^53 are exact in
- *           binary64).  A lane whose term is large, whose rounding is a tie,
- *           or whose result leaves the binade is instead subtracted alone
- *           with one IEEE subtraction, and the scan restarts after it.  The
- *           result equals the sequential loop bit for bit.
+ *           binary64).  When a step holds no codeword and no lane's term is
+ *           large, ties, or leaves the binade, only the step's total is needed
+ *           (a butterfly sum, exact for the same reason).  Otherwise a lane
+ *           whose term is large, whose rounding is a tie, or whose result
+ *           leaves the binade is subtracted alone with one IEEE subtraction,
+ *           and the scan restarts after it.  The result equals the sequential
+ *           loop bit for bit.
  *  list     codewords are taken in lane order; getLConf (:767-774) uses the
  *           running P_notGuess at each, so T and the list match exactly.
  *  output   soft output of :536-577 on lanes 0..15.
@@ -164,9 +167,90 @@ __device__ __forceinline__ bool sg_list_hit(SgListState& st, const SgLineParams&
     return conf > lp.thres || st.curl == lp.L;
 }
 
+/* Advance P_notGuess over lanes [0, nv) of one 32-pattern half (first pattern
+ * index bh) and take its codewords in order.  Within a binade the running
+ * value is an exact integer prefix sum (warp scan); a lane whose term is
+ * large, whose rounding ties or whose result leaves the binade is subtracted
+ * alone, and the scan restarts after it.  Sets T and done when the line
+ * decode stops. */
+__device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_t hits, int nv, uint32_t bh,
+                                                 double& P, SgListState& st, uint32_t& T, bool& done,
+                                                 const SgLineParams& lp, uint32_t hdm, int lane, int myrank)
+{
+    int s = 0;
+    while (s < nv && !done) {
+        if (!(P >= 0x1p-970)) { /* zero, negative, tiny or NaN: one lane alone */
+            const double es = __shfl_sync(SG_FULL, e, s);
+            P = __dsub_rn(P, es);
+            if ((hits >> s) & 1u) {
+                const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
+                if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
+                    T = bh + (uint32_t)s + 1u;
+                    done = true;
+                }
+            }
+            s++;
+            continue;
+        }
+        const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
+        const double u = sg_from_bits((uint64_t)(E - 52 + 1023) << 52);
+        const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
+        const double M0 = __dmul_rn(P, iu);
+        const bool mine = lane >= s && lane < nv;
+        const double q = mine ? __dmul_rn(e, iu) : 0.0;
+        const bool big = !(q < 0x1p52);
+        double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52); /* round(q), ties to even */
+        const bool tie = fabs(__dsub_rn(q, d)) == 0.5;
+        if (big)
+            d = 0.0;
+        double S = d;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double y = __shfl_up_sync(SG_FULL, S, off);
+            if (lane >= off)
+                S = __dadd_rn(S, y);
+        }
+        const double M = __dsub_rn(M0, S);
+        const uint32_t bm = __ballot_sync(SG_FULL, mine && (big || tie || !(M >= 0x1p52 + 1.0)));
+        const int f = bm ? __ffs(bm) - 1 : nv;
+        uint32_t hseg = hits & (f >= 32 ? SG_FULL : ((1u << f) - 1u)) & ~((1u << s) - 1u);
+        while (hseg) {
+            const int h = __ffs(hseg) - 1;
+            const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
+            const double eh = __shfl_sync(SG_FULL, e, h);
+            const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
+            if (sg_list_hit(st, lp, hdm, mj, Ph, eh, lane, myrank)) {
+                T = bh + (uint32_t)h + 1u;
+                done = true;
+                break;
+            }
+            hseg &= hseg - 1u;
+        }
+        if (done)
+            break;
+        if (f > s)
+            P = __dmul_rn(__shfl_sync(SG_FULL, M, f - 1), u);
+        if (f < nv) {
+            const double es = __shfl_sync(SG_FULL, e, f);
+            P = __dsub_rn(P, es);
+            if ((hits >> f) & 1u) {
+                const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
+                if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
+                    T = bh + (uint32_t)f + 1u;
+                    done = true;
+                }
+            }
+            s = f + 1;
+        } else {
+            s = nv;
+        }
+    }
+}
+
 /* Decode one line.  llr: this lane's input LLR (lanes 0..15; others
  * ignored).  enum_tabs: SG_ENUM_NTAB tables of SG_ENUM_LEN entries.
  * etab/ltab: shared-memory copies of the exp/log tables. */
+template <int G>
 __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineParams& lp,
                                                         const uint32_t* __restrict__ enum_tabs,
                                                         const double* etab, const double* ltab,
@@ -287,128 +371,99 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     st.curl = 0;
     uint32_t T = 0;
     bool done = false;
-    for (uint32_t base = 0; !done; base += 32) {
-        const uint32_t t = base + lane;
-        const uint32_t ent = __ldg(tab + (t < SG_ENUM_LEN ? t : SG_ENUM_LEN - 1u));
-        int nv = base + 32u <= SG_ENUM_LEN ? 32 : (int)(SG_ENUM_LEN - base);
+    for (uint32_t base = 0; !done; base += 32u * G) {
+        /* G patterns per lane: lane j of half h tests pattern base + 32h + j */
+        uint32_t ent[G];
+        double e[G];
+        uint32_t hits[G];
+        int nv[G];
+        int nvt = 0; /* valid patterns of the step, in order */
+#pragma unroll
+        for (int h = 0; h < G; h++) {
+            const uint32_t bh = base + 32u * h;
+            const uint32_t t = bh + lane;
+            ent[h] = __ldg(tab + (t < SG_ENUM_LEN ? t : SG_ENUM_LEN - 1u));
+            nv[h] = bh >= SG_ENUM_LEN ? 0 : (bh + 32u <= SG_ENUM_LEN ? 32 : (int)(SG_ENUM_LEN - bh));
+        }
         if (has_tmax) {
-            /* T < Tmax is checked before each new logistic weight (:652) */
-            const uint32_t cut =
-                __ballot_sync(SG_FULL, lane < nv && (ent & SG_ENUM_GS) && t > 0 && t >= lp.tmax);
-            if (cut)
-                nv = __ffs(cut) - 1;
+            /* T < Tmax is checked before each new logistic weight (:652); a cut
+             * in one half ends the step there */
+            bool cut_seen = false;
+#pragma unroll
+            for (int h = 0; h < G; h++) {
+                const uint32_t t = base + 32u * h + lane;
+                const uint32_t cut =
+                    __ballot_sync(SG_FULL, lane < nv[h] && (ent[h] & SG_ENUM_GS) && t > 0 && t >= lp.tmax);
+                if (cut_seen)
+                    nv[h] = 0;
+                else if (cut) {
+                    nv[h] = __ffs(cut) - 1;
+                    cut_seen = true;
+                }
+            }
         }
-        const uint32_t lim = nv >= 32 ? SG_FULL : ((1u << nv) - 1u);
-        const uint32_t lo = ent & 0xffu;
-        uint32_t hi = (ent >> 8) & 0xffu;
-        double pm = ws->A[lo];
-        const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
-        while (hi) {
-            pm = __dadd_rn(pm, ws->dhi[__ffs(hi) - 1]);
-            hi &= hi - 1u;
+#pragma unroll
+        for (int h = 0; h < G; h++) {
+            const uint32_t lo = ent[h] & 0xffu;
+            uint32_t hi = (ent[h] >> 8) & 0xffu;
+            double pm = ws->A[lo];
+            const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
+            while (hi) {
+                pm = __dadd_rn(pm, ws->dhi[__ffs(hi) - 1]);
+                hi &= hi - 1u;
+            }
+            e[h] = sg_exp_neg(-pm, etab);
+            hits[h] = __ballot_sync(SG_FULL, syn == 0u) & (nv[h] >= 32 ? SG_FULL : ((1u << nv[h]) - 1u));
+            nvt += nv[h];
         }
-        const double e = sg_exp_neg(-pm, etab);
-        const uint32_t hits = __ballot_sync(SG_FULL, syn == 0u) & lim;
 
         /* common case: no codeword, no large term, no tie and no binade
-         * crossing in the batch -- P_notGuess moves by the exact integer sum */
-        if (hits == 0u && P >= 0x1p-970) {
+         * crossing in the step -- P_notGuess moves by the exact integer sum */
+        bool any_hit = false;
+#pragma unroll
+        for (int h = 0; h < G; h++)
+            any_hit |= hits[h] != 0u;
+        if (!any_hit && P >= 0x1p-970) {
             const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
             const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
-            const double q = lane < nv ? __dmul_rn(e, iu) : 0.0;
-            const double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52);
-            const bool bad = !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
+            double dsum = 0.0;
+            bool bad = false;
+#pragma unroll
+            for (int h = 0; h < G; h++) {
+                const double q = lane < nv[h] ? __dmul_rn(e[h], iu) : 0.0;
+                const double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52);
+                bad |= !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
+                dsum = __dadd_rn(dsum, d); /* < 2^53 unless the step crosses anyway */
+            }
             if (!__any_sync(SG_FULL, bad)) {
-                double tot = d;
+                double tot = dsum;
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1)
                     tot = __dadd_rn(tot, __shfl_xor_sync(SG_FULL, tot, off));
                 const double M0 = __dmul_rn(P, iu);
                 if (tot <= __dsub_rn(M0, 0x1p52 + 1.0)) {
                     P = __dmul_rn(__dsub_rn(M0, tot), sg_from_bits((uint64_t)(E - 52 + 1023) << 52));
-                    T = base + (uint32_t)nv;
-                    if (nv < 32)
+                    T = base + (uint32_t)nvt;
+                    if (nvt < 32 * G)
                         done = true;
                     continue;
                 }
             }
         }
 
-        /* general case: advance P_notGuess over lanes [0, nv) in segments and
-         * take the codewords in order */
-        int s = 0;
-        while (s < nv && !done) {
-            if (!(P >= 0x1p-970)) { /* zero, negative, tiny or NaN: one lane alone */
-                const double es = __shfl_sync(SG_FULL, e, s);
-                P = __dsub_rn(P, es);
-                if ((hits >> s) & 1u) {
-                    const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
-                    if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
-                        T = base + (uint32_t)s + 1u;
-                        done = true;
-                    }
-                }
-                s++;
-                continue;
-            }
-            const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
-            const double u = sg_from_bits((uint64_t)(E - 52 + 1023) << 52);
-            const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
-            const double M0 = __dmul_rn(P, iu);
-            const bool mine = lane >= s && lane < nv;
-            const double q = mine ? __dmul_rn(e, iu) : 0.0;
-            const bool big = !(q < 0x1p52);
-            double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52); /* round(q), ties to even */
-            const bool tie = fabs(__dsub_rn(q, d)) == 0.5;
-            if (big)
-                d = 0.0;
-            double S = d;
+        /* general case, one half after the other */
 #pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const double y = __shfl_up_sync(SG_FULL, S, off);
-                if (lane >= off)
-                    S = __dadd_rn(S, y);
-            }
-            const double M = __dsub_rn(M0, S);
-            const uint32_t bm = __ballot_sync(SG_FULL, mine && (big || tie || !(M >= 0x1p52 + 1.0)));
-            const int f = bm ? __ffs(bm) - 1 : nv;
-            uint32_t hseg = hits & (f >= 32 ? SG_FULL : ((1u << f) - 1u)) & ~((1u << s) - 1u);
-            while (hseg) {
-                const int h = __ffs(hseg) - 1;
-                const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
-                const double eh = __shfl_sync(SG_FULL, e, h);
-                const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
-                if (sg_list_hit(st, lp, hdm, mj, Ph, eh, lane, myrank)) {
-                    T = base + (uint32_t)h + 1u;
-                    done = true;
-                    break;
-                }
-                hseg &= hseg - 1u;
-            }
+        for (int h = 0; h < G; h++) {
             if (done)
                 break;
-            if (f > s)
-                P = __dmul_rn(__shfl_sync(SG_FULL, M, f - 1), u);
-            if (f < nv) {
-                const double es = __shfl_sync(SG_FULL, e, f);
-                P = __dsub_rn(P, es);
-                if ((hits >> f) & 1u) {
-                    const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
-                    if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
-                        T = base + (uint32_t)f + 1u;
-                        done = true;
-                    }
-                }
-                s = f + 1;
-            } else {
-                s = nv;
+            sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, st, T, done, lp, hdm, lane, myrank);
+            if (!done && nv[h] < 32) {
+                T = base + 32u * h + (uint32_t)nv[h];
+                done = true;
             }
         }
-        if (!done) {
-            T = base + (uint32_t)nv;
-            if (nv < 32)
-                done = true;
-        }
+        if (!done)
+            T = base + 32u * G;
     }
 
     /* Soft output (:536-577) */
