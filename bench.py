@@ -309,6 +309,8 @@ def main():
                "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
                "api": "sg_decode_host (host buffers, copies inside the timed region)"}
 
+    ceil = C.c_double()
+    _lib.check(lib.sg_guess_ceiling(20000, C.byref(ceil)))
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -329,6 +331,11 @@ def main():
                        "l2": f"inputs ({n * 32768 / 1e9:.1f} GB per GPU) larger than L2; no flush"},
             "info_mbps": value * 512 / 1e6,
             "ber": ber, "ng_per_codeword": ng_per_cw, "guesses_per_s": value * ng_per_cw,
+            "guess_ceiling": {"bound": "fp64 exp per guess", "achieved": value * ng_per_cw / world,
+                              "peak": ceil.value, "unit": "guess/s per GPU",
+                              "frac": value * ng_per_cw / world / ceil.value,
+                              "how": "sg_guess_ceiling: PM add + exp(-PM) + P_notGuess subtract per guess, "
+                                     "all SMs, measured on this GPU in this run"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": None,
                          "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},

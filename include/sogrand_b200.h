@@ -209,6 +209,25 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
                             double ebn0_lo_db, double ebn0_hi_db, uint8_t* d_info,
                             double* d_llr, void* stream);
 
+/* ---- differentiation.  The soft output is piecewise smooth in the LLRs
+ * and the extrinsic weights: sorts, tested patterns, codeword lists, stops,
+ * early terminations and phase counts are held fixed as the branch of the
+ * forward pass.  sg_forward_device is sg_decode_device that also writes the
+ * L_E cube entering every phase, d_ckpt[n_cw][3*Imax][4096] (float64);
+ * sg_backward_device re-runs every line decode from those checkpoints in
+ * reverse phase order and returns, per codeword, the loss
+ *   sum_i softplus(s_i L_APP_i),  s_i = +1 for transmitted bit 1, -1 for 0
+ * (BCE of the final APP, over all 4096 code bits), its gradient with respect
+ * to the per-phase weights alpha (d_grad_alpha[n_cw][3*Imax]) and,
+ * optionally, to the channel LLRs (d_grad_llr[n_cw][4096]).  Requires
+ * Tmax >= 65536.  d_code_bits: [n_cw][4096] bytes 0/1 in cube order. */
+sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
+                            double* d_lapp, sg_cw_stats* d_stats, double* d_ckpt, void* stream);
+sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* p,
+                             const sg_cw_stats* d_stats, const double* d_ckpt,
+                             const uint8_t* d_code_bits, double* d_loss, double* d_grad_alpha,
+                             double* d_grad_llr, void* stream);
+
 /* ---- batched persistent decoder.  One resident CTA per SM holds several
  * codeword slots; warps take lines from any slot with work, the warp that
  * completes a phase runs early termination and either opens the slot's next
@@ -246,6 +265,13 @@ sg_status sg_decoder_set_variant(int v);
 int sg_decoder_get_variant(void);
 
 /* ---- diagnostics */
+
+/* Measured ceiling of the per-guess floating-point work on the current
+ * device: one path-metric addition, one exp(-PM) and one P_notGuess
+ * subtraction per guess, all SMs, no memory traffic; 2*iters guesses per
+ * thread.  Synchronous.  The decoder's guesses/s divided by this is its
+ * fraction of the arithmetic bound. */
+sg_status sg_guess_ceiling(unsigned long long iters, double* guesses_per_second);
 
 /* The order in which a line decode tests error patterns when its
  * reliability shift is IC (the loops of sogrand_main_logic,

@@ -189,6 +189,8 @@ typedef struct {
     int L;
     uint64_t Tmax;
     double thres;
+    double etot;          /* sum of exp(-PM) over the counted guesses */
+    double epos[SGO_N];   /* the same over guesses that flip position i */
 } line_state;
 
 /* PM of a test error pattern over sorted positions (getPM, D:765). */
@@ -221,7 +223,12 @@ static int visit(line_state* s, const uint8_t tep[SGO_N])
         c[s->perm[i]] = s->cHD[s->perm[i]] ^ tep[i];
     s->T += 1.0;
     double pm = pattern_pm(s, tep);
-    s->p_not_guess -= ox_exp(-pm);
+    double e = ox_exp(-pm);
+    s->p_not_guess -= e;
+    s->etot += e;
+    for (int i = 0; i < SGO_N; i++)
+        if (tep[i])
+            s->epos[s->perm[i]] += e;
     if (parity_ok(c)) {
         s->pm_list[s->cur_l] = pm;
         memcpy(s->chat[s->cur_l], c, SGO_N);
@@ -337,6 +344,9 @@ static void main_logic(line_state* s, const double llr[SGO_N])
     s->cur_l = 0;
     s->pnl = 0.0;
     s->p_not_guess = 1.0;
+    s->etot = 0.0;
+    for (int i = 0; i < n; i++)
+        s->epos[i] = 0.0;
     double pm = 0;
     for (int i = 0; i < n; i++) /* getPM_HD before sorting, D:617, D:764 */
         pm += jaclog(-s->absL[i]);
@@ -393,8 +403,18 @@ size_t sgo_pattern_order(int32_t ic, uint32_t* out, size_t cap)
 double sgo_exp(double x) { return ox_exp(x); }
 double sgo_log(double x) { return ox_log(x); }
 
+static void bitso_state(const double llr[SGO_N], int L, uint64_t Tmax, double thres, sgo_line_out* out,
+                        line_state* sp);
+
 /* Soft output of one line (SOGRAND_bitSO, D:521-585). */
 void sgo_bitso(const double llr[SGO_N], int L, uint64_t Tmax, double thres, sgo_line_out* out)
+{
+    line_state s;
+    bitso_state(llr, L, Tmax, thres, out, &s);
+}
+
+static void bitso_state(const double llr[SGO_N], int L, uint64_t Tmax, double thres, sgo_line_out* out,
+                        line_state* sp)
 {
     code_init();
     line_state s;
@@ -405,6 +425,7 @@ void sgo_bitso(const double llr[SGO_N], int L, uint64_t Tmax, double thres, sgo_
     out->n_guess = (uint64_t)s.T;
     out->cur_l = s.cur_l;
     out->pnl = s.pnl;
+    *sp = s;
     if (s.cur_l == 0) {
         /* The reference reads an uninitialised list size here (D:524, D:536);
          * it is unreachable with Tmax = UINT64_MAX.  The defined behaviour is
@@ -617,6 +638,172 @@ void sgo_decode(const double* llr, size_t n_cw, const sgo_params* p,
     free(lapp);
     free(le);
     free(input);
+}
+
+/* ------------------------------------------------------------ adjoint -- */
+
+/* Transpose of d L_APP / d x of one line on the forward branch (the list,
+ * the tested patterns and the stop held fixed), applied to g.  The soft
+ * output is that of D:536-577; PM_j = sum_k JacLog(-|x_k|) + sum over the
+ * positions where pattern j differs from the hard decision of
+ * (JacLog(|x_k|) - JacLog(-|x_k|)), so dPM_j/dx_i = sign(x_i) ([i in S_j] -
+ * sigma(-|x_i|) [|x_i| <= 50]); pNL = 2^-8 (1 - sum of exp(-PM) over the
+ * counted guesses). */
+static void line_vjp(const double x[SGO_N], const double g[SGO_N], const line_state* s, double gx[SGO_N])
+{
+    if (s->cur_l == 0) {
+        for (int i = 0; i < SGO_N; i++)
+            gx[i] = g[i];
+        return;
+    }
+    const double eps = kEps;
+    const int pnl_live = s->pnl > eps;
+    const double p_nl = fmax(s->pnl, eps);
+    double pj[8], a0[SGO_N], a1[SGO_N], pp0[SGO_N], pp1[SGO_N], sgn[SGO_N], sm[SGO_N];
+    for (int j = 0; j < s->cur_l; j++)
+        pj[j] = ox_exp(-s->pm_list[j]);
+    for (int i = 0; i < SGO_N; i++) {
+        const double pp1r = 1.0 / (1.0 + ox_exp(x[i]));
+        const double pp0r = 1.0 - pp1r;
+        pp1[i] = fmin(fmax(pp1r, eps), 1.0);
+        pp0[i] = fmin(fmax(pp0r, eps), 1.0);
+        double p0 = 0, p1 = 0;
+        for (int j = 0; j < s->cur_l; j++) {
+            if (s->chat[j][i])
+                p1 += pj[j];
+            else
+                p0 += pj[j];
+        }
+        p0 += p_nl * pp0[i];
+        p1 += p_nl * pp1[i];
+        a0[i] = p0 > eps ? g[i] / p0 : 0.0;
+        a1[i] = p1 > eps ? -g[i] / p1 : 0.0;
+        const double dsig = pp0r * pp1r;
+        gx[i] = 0.0;
+        if (pp0r > eps)
+            gx[i] += a0[i] * p_nl * dsig;
+        if (pp1r > eps)
+            gx[i] -= a1[i] * p_nl * dsig;
+        const double ax = fabs(x[i]);
+        sgn[i] = x[i] > 0 ? 1.0 : (x[i] < 0 ? -1.0 : 0.0);
+        sm[i] = ax <= 50.0 ? 1.0 / (1.0 + ox_exp(ax)) : 0.0;
+    }
+    for (int j = 0; j < s->cur_l; j++) {
+        double gp = 0;
+        for (int i = 0; i < SGO_N; i++)
+            gp += s->chat[j][i] ? a1[i] : a0[i];
+        const double gpm = -pj[j] * gp;
+        for (int i = 0; i < SGO_N; i++) {
+            const double inS = (s->chat[j][i] != s->cHD[i]) ? 1.0 : 0.0;
+            gx[i] += gpm * sgn[i] * (inS - sm[i]);
+        }
+    }
+    if (pnl_live) {
+        double gpnl = 0;
+        for (int i = 0; i < SGO_N; i++)
+            gpnl += a0[i] * pp0[i] + a1[i] * pp1[i];
+        for (int i = 0; i < SGO_N; i++)
+            gx[i] += gpnl * 0x1p-8 * sgn[i] * (s->epos[i] - sm[i] * s->etot);
+    }
+}
+
+static double softplus(double z) { return z > 0 ? z + log1p(exp(-z)) : log1p(exp(z)); }
+
+void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, double* loss_out,
+                        double* grad_alpha, double* grad_llr)
+{
+    code_init();
+    static const int stride[3] = {1, 16, 256};
+    const int nph = 3 * p->Imax;
+    double* ck = (double*)calloc((size_t)nph * SGO_CUBE, sizeof(double));
+    double* le = (double*)calloc(SGO_CUBE, sizeof(double));
+    double* lapp = (double*)calloc(SGO_CUBE, sizeof(double));
+    double* gle = (double*)calloc(SGO_CUBE, sizeof(double));
+    int P = 0;
+    /* forward (sgo_decode's loop) with a checkpoint of L_E entering each phase */
+    for (int ph = 0; ph < nph; ph++) {
+        const int axis = ph % 3;
+        memcpy(ck + (size_t)ph * SGO_CUBE, le, sizeof(double) * SGO_CUBE);
+        for (int a = 0; a < SGO_N; a++)
+            for (int b = 0; b < SGO_N; b++) {
+                const int base = axis == 0 ? IDX(0, b, a) : axis == 1 ? IDX(b, 0, a) : IDX(b, a, 0);
+                double v[SGO_N];
+                for (int i = 0; i < SGO_N; i++) {
+                    const int q = base + i * stride[axis];
+                    double la = p->alpha[ph] * ck[(size_t)ph * SGO_CUBE + q];
+                    v[i] = llr[q] + la;
+                }
+                sgo_line_out o;
+                sgo_bitso(v, p->L, p->Tmax, p->thres, &o);
+                for (int i = 0; i < SGO_N; i++) {
+                    lapp[base + i * stride[axis]] = o.lapp[i];
+                    le[base + i * stride[axis]] = o.le[i];
+                }
+            }
+        P = ph + 1;
+        if (sgo_early_termination(lapp))
+            break;
+    }
+    /* backward */
+    double loss = 0;
+    for (int ph = 0; ph < nph; ph++)
+        grad_alpha[ph] = 0;
+    for (int i = 0; i < SGO_CUBE; i++)
+        grad_llr[i] = 0;
+    for (int ph = P - 1; ph >= 0; ph--) {
+        const int axis = ph % 3;
+        const double* lep = ck + (size_t)ph * SGO_CUBE;
+        for (int a = 0; a < SGO_N; a++)
+            for (int b = 0; b < SGO_N; b++) {
+                const int base = axis == 0 ? IDX(0, b, a) : axis == 1 ? IDX(b, 0, a) : IDX(b, a, 0);
+                double v[SGO_N], g[SGO_N], gE[SGO_N], gx[SGO_N];
+                for (int i = 0; i < SGO_N; i++) {
+                    const int q = base + i * stride[axis];
+                    double la = p->alpha[ph] * lep[q];
+                    v[i] = llr[q] + la;
+                }
+                sgo_line_out o;
+                line_state st;
+                bitso_state(v, p->L, p->Tmax, p->thres, &o, &st);
+                for (int i = 0; i < SGO_N; i++) {
+                    const int q = base + i * stride[axis];
+                    gE[i] = gle[q];
+                    g[i] = gE[i];
+                    if (ph == P - 1) {
+                        const double sg = code_bits[q] ? 1.0 : -1.0;
+                        const double z = sg * o.lapp[i];
+                        loss += softplus(z);
+                        g[i] += sg / (1.0 + exp(-z));
+                    }
+                }
+                line_vjp(v, g, &st, gx);
+                for (int i = 0; i < SGO_N; i++) {
+                    const int q = base + i * stride[axis];
+                    gx[i] -= gE[i];
+                    gle[q] = p->alpha[ph] * gx[i];
+                    grad_alpha[ph] += gx[i] * lep[q];
+                    grad_llr[q] += gx[i];
+                }
+            }
+    }
+    *loss_out = loss;
+    free(ck);
+    free(le);
+    free(lapp);
+    free(gle);
+}
+
+/* Loss of the forward pass alone (for finite differences). */
+double sgo_decode_loss(const double* llr, const sgo_params* p, const uint8_t* code_bits)
+{
+    double* lapp = (double*)malloc(sizeof(double) * SGO_CUBE);
+    uint8_t bits[SGO_INFO / 8];
+    sgo_decode(llr, 1, p, bits, lapp, NULL);
+    double loss = 0;
+    for (int i = 0; i < SGO_CUBE; i++)
+        loss += softplus((code_bits[i] ? 1.0 : -1.0) * lapp[i]);
+    free(lapp);
+    return loss;
 }
 
 double sgo_sigma(double ebn0_db) /* C:34-39, code_dim = 3 */

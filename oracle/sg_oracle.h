@@ -81,6 +81,14 @@ void sgo_encode(const uint8_t info[SGO_INFO], uint8_t cw[SGO_CUBE]);
 /* Noise standard deviation of channel_sim.c:34-39 for code dimension 3. */
 double sgo_sigma(double ebn0_db);
 
+/* FP64 adjoint of one codeword's decode (the branch of the forward pass
+ * held fixed): loss = sum_i softplus(s_i L_APP_i) over the 4096 code bits,
+ * s_i = +1 for bit 1, -1 for 0; grad_alpha[3*Imax] and grad_llr[4096] its
+ * gradients.  Requires Tmax = UINT64_MAX. */
+void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, double* loss,
+                        double* grad_alpha, double* grad_llr);
+double sgo_decode_loss(const double* llr, const sgo_params* p, const uint8_t* code_bits);
+
 /* Which exp/log this build uses: 0 = libm, 1 = sg_math.h. */
 int sgo_math_mode(void);
 

@@ -54,6 +54,7 @@ struct SgDecodeArgs {
     sg_cw_stats* stats;
     const uint32_t* enum_tabs;
     unsigned int* err;
+    double* ckpt; /* nullable: [n_cw][3*imax][4096], L_E entering each phase */
     unsigned long long n_cw;
     int32_t L;
     int32_t imax;
@@ -241,8 +242,11 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
                         break;
                     const int pos = sg_pos(axis, l, lane & 15);
                     double v = 1.0;
-                    if (lane < 16) /* L_ch + (alpha*L_E) */
+                    if (lane < 16) { /* L_ch + (alpha*L_E) */
                         v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, S.le[pos]));
+                        if (args.ckpt)
+                            args.ckpt[(cw * (3ull * args.imax) + 3 * (iter - 1) + axis) * SG_CUBE + pos] = S.le[pos];
+                    }
                     const SgLineResult r =
                         sg_decode_line<G>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
                     if (lane < 16) {
@@ -306,6 +310,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
 }
 
 #include "sg_persist.cuh"
+#include "sg_adjoint.cuh"
 
 struct SgLineSmem {
     alignas(16) double etab[SG_EXP_TAB_LEN];
@@ -536,6 +541,28 @@ __global__ void sg_enum_build_kernel(uint32_t* out, unsigned int* ok)
         ok[ic] = sg_enum_build_impl(ic, out + (size_t)ic * SG_ENUM_LEN) == SG_ENUM_LEN ? 1u : 0u;
 }
 
+/* Ceiling of the per-guess floating-point work: each thread evaluates, per
+ * iteration, one path-metric addition, exp(-PM) (sg_exp_neg, the guess
+ * loop's routine) and one P_notGuess subtraction, with no memory traffic
+ * beyond the shared exp table.  guesses/s of this kernel over all SMs bounds
+ * what any decoder with the reference's per-guess arithmetic can reach. */
+__global__ void __launch_bounds__(256) sg_guess_ceiling_kernel(unsigned long long iters, double* sink)
+{
+    __shared__ alignas(16) double etab[SG_EXP_TAB_LEN];
+    for (int i = threadIdx.x; i < SG_EXP_TAB_LEN; i += 256)
+        etab[i] = g_etab[i];
+    __syncthreads();
+    double pm0 = 1e-3 * (threadIdx.x + 1), pm1 = pm0 + 0.37, acc0 = 1.0, acc1 = 1.0;
+    for (unsigned long long k = 0; k < iters; k++) {
+        pm0 = __dadd_rn(pm0, 1.1e-5);
+        pm1 = __dadd_rn(pm1, 1.3e-5);
+        acc0 = __dsub_rn(acc0, sg_exp_neg(-pm0, etab));
+        acc1 = __dsub_rn(acc1, sg_exp_neg(-pm1, etab));
+    }
+    if (acc0 + acc1 == 12345.0)
+        sink[blockIdx.x] = acc0;
+}
+
 /* -------------------------------------------------------------- host -- */
 
 namespace {
@@ -564,6 +591,7 @@ struct DevCtx {
     bool ready = false;
     uint32_t* enum_tabs = nullptr;
     unsigned int* err = nullptr;
+    double* err_sink = nullptr; /* never-read output of the ceiling kernel */
     int sms = 0;
 };
 
@@ -607,6 +635,7 @@ sg_status get_ctx(DevCtx** out)
         SG_CUDA(cudaMalloc(&c.enum_tabs, bytes));
         SG_CUDA(cudaMemcpy(c.enum_tabs, g_enum_host.data(), bytes, cudaMemcpyHostToDevice));
         SG_CUDA(cudaMalloc(&c.err, sizeof(unsigned int)));
+        SG_CUDA(cudaMalloc(&c.err_sink, 148 * 64 * sizeof(double)));
         SG_CUDA(cudaMemset(c.err, 0, sizeof(unsigned int)));
         SG_CUDA(cudaMemcpyToSymbol(c_hcol, g_code.hcol, sizeof g_code.hcol));
         SG_CUDA(cudaMemcpyToSymbol(c_prow, g_code.prow, sizeof g_code.prow));
@@ -617,6 +646,8 @@ sg_status get_ctx(DevCtx** out)
         for (int v = 0; v < SG_NPVARIANTS; v++)
             SG_CUDA(cudaFuncSetAttribute(g_pvariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)g_pvariants[v].smem));
+        SG_CUDA(cudaFuncSetAttribute(sg_backward_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(SgBackSmem<8>)));
         SG_CUDA(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
         c.ready = true;
     }
@@ -1314,6 +1345,107 @@ sg_status sg_batch_set_variant(int v)
 }
 
 int sg_batch_get_variant(void) { return g_pvariant; }
+
+sg_status sg_guess_ceiling(unsigned long long iters, double* guesses_per_second)
+{
+    if (!guesses_per_second || iters == 0)
+        return fail(SG_ERR_ARG, "need iters > 0 and an output pointer");
+    DevCtx* c = nullptr;
+    sg_status s = get_ctx(&c);
+    if (s != SG_OK)
+        return s;
+    const int blocks = c->sms * 8; /* 8 CTAs x 8 warps per SM */
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SG_CUDA(cudaEventCreate(&e0));
+    SG_CUDA(cudaEventCreate(&e1));
+    sg_guess_ceiling_kernel<<<blocks, 256>>>(iters / 8 + 1, c->err_sink); /* warm-up */
+    SG_CUDA(cudaEventRecord(e0));
+    sg_guess_ceiling_kernel<<<blocks, 256>>>(iters, c->err_sink);
+    SG_CUDA(cudaEventRecord(e1));
+    SG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    SG_CUDA(cudaGetLastError());
+    *guesses_per_second = 2.0 * (double)iters * blocks * 256 / (ms / 1000.0);
+    return SG_OK;
+}
+
+sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits, double* d_lapp,
+                            sg_cw_stats* d_stats, double* d_ckpt, void* stream)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (n_cw == 0)
+        return SG_OK;
+    if (!d_llr || !d_bits || !d_stats || !d_ckpt)
+        return fail(SG_ERR_ARG, "llr, bits, stats and ckpt must not be NULL");
+    if ((uintptr_t)d_llr & 7u)
+        return fail(SG_ERR_ARG, "llr must be 8-byte aligned");
+    DevCtx* c = nullptr;
+    if ((s = get_ctx(&c)) != SG_OK)
+        return s;
+    SgDecodeArgs a;
+    memset(&a, 0, sizeof a);
+    a.llr = d_llr;
+    a.bits = d_bits;
+    a.lapp = d_lapp;
+    a.stats = d_stats;
+    a.enum_tabs = c->enum_tabs;
+    a.err = c->err;
+    a.ckpt = d_ckpt;
+    a.n_cw = n_cw;
+    a.L = p->L;
+    a.imax = p->Imax;
+    a.tmax = tmax_eff(p->Tmax);
+    a.use_bulk = ((uintptr_t)d_llr & 15u) == 0;
+    a.thres = p->thres;
+    memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    const SgVariant& v = g_variants[g_variant];
+    void* kargs[] = {(void*)&a};
+    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid_for(n_cw, 1 << 30)), dim3(v.nw * 32), kargs, v.smem,
+                             (cudaStream_t)stream));
+    return SG_OK;
+}
+
+sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* p, const sg_cw_stats* d_stats,
+                             const double* d_ckpt, const uint8_t* d_code_bits, double* d_loss,
+                             double* d_grad_alpha, double* d_grad_llr, void* stream)
+{
+    sg_status s = check_params(p);
+    if (s != SG_OK)
+        return s;
+    if (p->Tmax < SG_ENUM_LEN && p->Tmax != 0)
+        return fail(SG_ERR_ARG, "the adjoint needs Tmax >= 65536 (every line stops at a list insertion)");
+    if (n_cw == 0)
+        return SG_OK;
+    if (!d_llr || !d_stats || !d_ckpt || !d_code_bits || !d_loss || !d_grad_alpha)
+        return fail(SG_ERR_ARG, "NULL buffer");
+    DevCtx* c = nullptr;
+    if ((s = get_ctx(&c)) != SG_OK)
+        return s;
+    SgBackwardArgs a;
+    memset(&a, 0, sizeof a);
+    a.llr = d_llr;
+    a.ckpt = d_ckpt;
+    a.stats = d_stats;
+    a.code_bits = d_code_bits;
+    a.enum_tabs = c->enum_tabs;
+    a.loss = d_loss;
+    a.grad_alpha = d_grad_alpha;
+    a.grad_llr = d_grad_llr;
+    a.n_cw = n_cw;
+    a.L = p->L;
+    a.nph = 3 * p->Imax;
+    a.thres = p->thres;
+    memcpy(a.alpha, p->alpha, sizeof a.alpha);
+    void* kargs[] = {(void*)&a};
+    SG_CUDA(cudaLaunchKernel((const void*)sg_backward_kernel<8>, dim3(grid_for(n_cw, 1 << 30)), dim3(256), kargs,
+                             sizeof(SgBackSmem<8>), (cudaStream_t)stream));
+    return SG_OK;
+}
 
 int sg_decoder_variant_count(void) { return SG_NVARIANTS; }
 

@@ -247,14 +247,28 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
     }
 }
 
+/* Extra results of a line decode run for the adjoint (ADJ = true): the
+ * sums over the counted guesses that P_notGuess depends on, and the list.
+ * Valid for decodes that stop at a list insertion (Tmax >= 65536). */
+struct SgAdjOut {
+    double etot;    /* uniform: sum of exp(-PM) over the counted guesses */
+    double esort;   /* lane r < 16: the same sum over guesses whose pattern holds sorted position r */
+    double pnl;     /* uniform: pNL of the last list insertion (before the 1e-40 clamp) */
+    double my_e;    /* lane k < curl: exp(-PM) of list entry k */
+    uint32_t my_cm; /* lane k < curl: bits of list entry k */
+    uint32_t hdm;   /* hard decision, bit i = position i */
+    int32_t curl;
+    int32_t myrank; /* lane i < 16: sorted rank of position i */
+};
+
 /* Decode one line.  llr: this lane's input LLR (lanes 0..15; others
  * ignored).  enum_tabs: SG_ENUM_NTAB tables of SG_ENUM_LEN entries.
  * etab/ltab: shared-memory copies of the exp/log tables. */
-template <int G>
+template <int G, bool ADJ = false>
 __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineParams& lp,
                                                         const uint32_t* __restrict__ enum_tabs,
                                                         const double* etab, const double* ltab,
-                                                        SgWarpScratch* ws)
+                                                        SgWarpScratch* ws, SgAdjOut* adj = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const bool act = lane < 16;
@@ -371,6 +385,10 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     st.curl = 0;
     uint32_t T = 0;
     bool done = false;
+    double adj_tot = 0.0, adj_r[ADJ ? 16 : 1];
+#pragma unroll
+    for (int r = 0; r < (ADJ ? 16 : 1); r++)
+        adj_r[r] = 0.0;
     for (uint32_t base = 0; !done; base += 32u * G) {
         /* G patterns per lane: lane j of half h tests pattern base + 32h + j */
         uint32_t ent[G];
@@ -419,7 +437,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
         /* common case: no codeword, no large term, no tie and no binade
          * crossing in the step -- P_notGuess moves by the exact integer sum */
-        bool any_hit = false;
+        bool any_hit = false, stepped = false;
 #pragma unroll
         for (int h = 0; h < G; h++)
             any_hit |= hits[h] != 0u;
@@ -446,24 +464,63 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                     T = base + (uint32_t)nvt;
                     if (nvt < 32 * G)
                         done = true;
-                    continue;
+                    stepped = true;
                 }
             }
         }
 
         /* general case, one half after the other */
+        if (!stepped) {
 #pragma unroll
-        for (int h = 0; h < G; h++) {
-            if (done)
-                break;
-            sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, st, T, done, lp, hdm, lane, myrank);
-            if (!done && nv[h] < 32) {
-                T = base + 32u * h + (uint32_t)nv[h];
-                done = true;
+            for (int h = 0; h < G; h++) {
+                if (done)
+                    break;
+                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, st, T, done, lp, hdm, lane,
+                                 myrank);
+                if (!done && nv[h] < 32) {
+                    T = base + 32u * h + (uint32_t)nv[h];
+                    done = true;
+                }
+            }
+            if (!done)
+                T = base + 32u * G;
+        }
+        if (ADJ) {
+            /* the guesses of this step that entered P_notGuess: [base, T) */
+#pragma unroll
+            for (int h = 0; h < G; h++) {
+                if (base + 32u * h + (uint32_t)lane < T) {
+                    adj_tot += e[h];
+                    const uint32_t m = ent[h] & 0xffffu;
+#pragma unroll
+                    for (int r = 0; r < (ADJ ? 16 : 1); r++)
+                        if ((m >> r) & 1u)
+                            adj_r[r] += e[h];
+                }
             }
         }
-        if (!done)
-            T = base + 32u * G;
+    }
+    if (ADJ) {
+        /* sums over the warp; lane r keeps sorted position r */
+        for (int off = 16; off > 0; off >>= 1)
+            adj_tot += __shfl_xor_sync(SG_FULL, adj_tot, off);
+        double mine_r = 0.0;
+#pragma unroll
+        for (int r = 0; r < (ADJ ? 16 : 1); r++) {
+            double v = adj_r[r];
+            for (int off = 16; off > 0; off >>= 1)
+                v += __shfl_xor_sync(SG_FULL, v, off);
+            if (lane == r)
+                mine_r = v;
+        }
+        adj->etot = adj_tot;
+        adj->esort = mine_r;
+        adj->pnl = st.pnl;
+        adj->my_e = st.my_e;
+        adj->my_cm = st.my_cm;
+        adj->hdm = hdm;
+        adj->curl = st.curl;
+        adj->myrank = myrank;
     }
 
     /* Soft output (:536-577) */

@@ -1,0 +1,166 @@
+"""Differentiable decoding: torch.autograd.Function over the C ABI pair
+sg_forward_device / sg_backward_device, and learning of the per-phase
+extrinsic weights.
+
+The reference scales the extrinsic information with one constant, alpha =
+0.7 for every phase (SOGRAND_C/cubic_decoder_final.c:100-102).  Here the
+3*Imax per-phase weights are trainable: the loss is the BCE of the final
+APP against the transmitted code bits,
+    loss = mean over codewords of sum_i softplus(s_i L_APP_i),  s_i = 2 c_i - 1,
+differentiated exactly on the branch of the forward pass (sorts, tested
+patterns, lists, stops, early terminations held fixed).  The plain decoder
+with the learned weights is then judged by BER.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+def _params(alpha_np, imax: int, L: int):
+    import sogrand_b200 as sg
+
+    a = np.full(sg.SG_MAX_PHASES, 0.7)
+    a[: 3 * imax] = alpha_np[: 3 * imax]
+    return sg.params(L=L, Imax=imax, alpha=a)
+
+
+def _torch_fn():
+    import torch
+
+    class DecodeBCE(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, alpha, llr, code_bits, imax: int, L: int):
+            import sogrand_b200 as sg
+
+            lib = _lib.load()
+            n = llr.shape[0]
+            nph = 3 * imax
+            dev = llr.device
+            p = _params(alpha.detach().cpu().numpy(), imax, L)
+            ckpt = torch.empty((n, nph, sg.SG_CUBE), dtype=torch.float64, device=dev)
+            bits = torch.empty((n, sg.SG_INFO_BYTES), dtype=torch.uint8, device=dev)
+            stats = torch.empty((n, sg.STATS_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+            lapp = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev)
+            s = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(lib.sg_forward_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), lapp.data_ptr(),
+                                             stats.data_ptr(), ckpt.data_ptr(), s))
+            sgn = code_bits.to(torch.float64) * 2.0 - 1.0
+            loss = torch.nn.functional.softplus(sgn * lapp).sum(dim=1).mean()
+            ctx.save_for_backward(llr, code_bits, ckpt, stats)
+            ctx.p = p
+            ctx.imax = imax
+            ctx.want_llr = llr.requires_grad
+            ctx.bits = bits
+            return loss
+
+        @staticmethod
+        def backward(ctx, g):
+            import sogrand_b200 as sg
+
+            llr, code_bits, ckpt, stats = ctx.saved_tensors
+            lib = _lib.load()
+            n = llr.shape[0]
+            nph = 3 * ctx.imax
+            dev = llr.device
+            loss = torch.empty(n, dtype=torch.float64, device=dev)
+            ga = torch.empty((n, nph), dtype=torch.float64, device=dev)
+            gl = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev) if ctx.want_llr else None
+            s = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(lib.sg_backward_device(llr.data_ptr(), n, C.byref(ctx.p), stats.data_ptr(),
+                                              ckpt.data_ptr(), code_bits.data_ptr(), loss.data_ptr(),
+                                              ga.data_ptr(), gl.data_ptr() if gl is not None else None, s))
+            grad_alpha = g * ga.sum(dim=0) / n
+            grad_llr = g * gl / n if gl is not None else None
+            return grad_alpha, grad_llr, None, None, None
+
+    return DecodeBCE
+
+
+_FN = None
+
+
+def decode_bce(alpha, llr, code_bits, imax: int = 30, L: int = 3):
+    """Mean BCE of the final APP over codewords; differentiable in alpha
+    (float64 tensor of 3*imax weights) and in llr (CUDA [n, 4096] float64).
+    code_bits: CUDA uint8 [n, 4096] transmitted bits."""
+    global _FN
+    if _FN is None:
+        _FN = _torch_fn()
+    return _FN.apply(alpha, llr, code_bits.contiguous(), imax, L)
+
+
+def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False):
+    """Per-codeword loss and gradients from sg_backward_device (CUDA tensors)."""
+    import torch
+
+    import sogrand_b200 as sg
+
+    n = llr.shape[0]
+    nph = 3 * p.Imax
+    dev = llr.device
+    loss = torch.empty(n, dtype=torch.float64, device=dev)
+    ga = torch.empty((n, nph), dtype=torch.float64, device=dev)
+    gl = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev) if want_llr else None
+    _lib.check(_lib.load().sg_backward_device(llr.data_ptr(), n, C.byref(p), stats.data_ptr(), ckpt.data_ptr(),
+                                              code_bits.data_ptr(), loss.data_ptr(), ga.data_ptr(),
+                                              gl.data_ptr() if gl is not None else None,
+                                              torch.cuda.current_stream(dev).cuda_stream))
+    return loss, ga, gl
+
+
+def forward_raw(llr, p):
+    """sg_forward_device: (bits, raw stats, lapp, checkpoints)."""
+    import torch
+
+    import sogrand_b200 as sg
+
+    n = llr.shape[0]
+    dev = llr.device
+    ckpt = torch.empty((n, 3 * p.Imax, sg.SG_CUBE), dtype=torch.float64, device=dev)
+    bits = torch.empty((n, sg.SG_INFO_BYTES), dtype=torch.uint8, device=dev)
+    stats = torch.empty((n, sg.STATS_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    lapp = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev)
+    _lib.check(_lib.load().sg_forward_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), lapp.data_ptr(),
+                                             stats.data_ptr(), ckpt.data_ptr(),
+                                             torch.cuda.current_stream(dev).cuda_stream))
+    return bits, stats, lapp, ckpt
+
+
+def code_bits_for(info, device):
+    """Transmitted code bits [n, 4096] (uint8, CUDA) of packed info blocks."""
+    import torch
+
+    import sogrand_b200 as sg
+
+    info_np = info.cpu().numpy() if hasattr(info, "cpu") else np.asarray(info)
+    return torch.from_numpy(sg.encode(info_np)).to(device)
+
+
+def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax: int = 30, lr: float = 0.02,
+                  seed: int = 90210, device: str = "cuda", init: float = 0.7, log=None):
+    """Adam on the 3*imax extrinsic weights over fresh seeded batches (each
+    step a new range of the codeword stream).  Returns (weights, history)."""
+    import torch
+
+    import sogrand_b200 as sg
+
+    alpha = torch.full((3 * imax,), init, dtype=torch.float64, device=device, requires_grad=True)
+    opt = torch.optim.Adam([alpha], lr=lr)
+    hist = []
+    for step in range(steps):
+        info, llr = sg.gen_llr(seed, step * batch, batch, ebn0_db=ebn0_db, device=device)
+        cb = code_bits_for(info, device)
+        opt.zero_grad()
+        loss = decode_bce(alpha, llr, cb, imax)
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            alpha.clamp_(0.0, 2.0)
+        hist.append(float(loss.item()))
+        if log:
+            log(step, hist[-1])
+    return alpha.detach().cpu().numpy(), hist
