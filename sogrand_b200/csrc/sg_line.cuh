@@ -278,7 +278,11 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     /* HardDec (:758): 1 unless llr > 0 */
     const uint32_t hdm = __ballot_sync(SG_FULL, act && !(llr > 0.0)) & 0xffffu;
     /* JacLog(-|L_i|) for getPM_HD (:617, :764) */
-    const double jn = act ? sg_jaclog(-a, etab, ltab) : 0.0;
+    /* lanes 0..15: JacLog(-|L_i|); lanes 16..31: JacLog(+|L_(lane-16)|), used
+     * for the sorted PM increments below */
+    const double a_all = __shfl_sync(SG_FULL, a, lane & 15);
+    const double jl = sg_jaclog(act ? -a_all : a_all, etab, ltab);
+    const double jn = act ? jl : 0.0;
 
     /* QuickSort of |L| ascending (:618) */
     int lt = 0, eq = 0;
@@ -322,7 +326,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
     /* PM increment of each sorted position (getPM, :765) and its syndrome */
     const double jn_src = __shfl_sync(SG_FULL, jn, src);
-    const double dl = act ? __dsub_rn(sg_jaclog(as, etab, ltab), jn_src) : 0.0;
+    const double jp_src = __shfl_sync(SG_FULL, jl, 16 + src); /* JacLog(|L|) of the same position */
+    const double dl = act ? __dsub_rn(jp_src, jn_src) : 0.0;
     const uint32_t hs = act ? c_hcol[src] : 0u;
     /* syndrome of the hard decision */
     const uint32_t s0 = __reduce_xor_sync(SG_FULL, (act && ((hdm >> lane) & 1u)) ? (uint32_t)c_hcol[lane] : 0u);
@@ -532,21 +537,26 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         lapp = llr;
         le = 0.0;
     } else {
+        /* every lane works on position lane & 15; lanes 0..15 then take
+         * log(p0), lanes 16..31 log(p1) */
+        const int pos = lane & 15;
+        const double x = __shfl_sync(SG_FULL, llr, pos);
         const double pnlc = fmax(st.pnl, 1e-40);
-        double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, sg_exp(llr, etab)));
+        double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, sg_exp(x, etab)));
         double pp0 = __dsub_rn(1.0, pp1);
         pp1 = fmin(fmax(pp1, 1e-40), 1.0);
         pp0 = fmin(fmax(pp0, 1e-40), 1.0);
         double p1 = 0.0, p0 = 0.0;
         for (int j = 0; j < st.curl; j++) {
-            const double c = (double)((__shfl_sync(SG_FULL, st.my_cm, j) >> lane) & 1u);
+            const double c = (double)((__shfl_sync(SG_FULL, st.my_cm, j) >> pos) & 1u);
             const double pj = __shfl_sync(SG_FULL, st.my_e, j);
             p1 = __dadd_rn(p1, __dmul_rn(c, pj));
             p0 = __dadd_rn(p0, __dmul_rn(__dsub_rn(1.0, c), pj));
         }
         p0 = __dadd_rn(p0, __dmul_rn(pnlc, pp0));
         p1 = __dadd_rn(p1, __dmul_rn(pnlc, pp1));
-        lapp = __dsub_rn(sg_log(fmax(p0, 1e-40), ltab), sg_log(fmax(p1, 1e-40), ltab));
+        const double lg = sg_log(fmax(act ? p0 : p1, 1e-40), ltab);
+        lapp = __dsub_rn(lg, __shfl_sync(SG_FULL, lg, (lane & 15) + 16));
         le = __dsub_rn(lapp, llr);
     }
     res.lapp = lapp;

@@ -141,16 +141,37 @@ def code_bits_for(info, device):
 
 
 def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax: int = 30, lr: float = 0.02,
-                  seed: int = 90210, device: str = "cuda", init: float = 0.7, log=None):
+                  seed: int = 90210, device: str = "cuda", init: float = 0.7, log=None, val_cw: int = 0,
+                  val_every: int = 10):
     """Adam on the 3*imax extrinsic weights over fresh seeded batches (each
-    step a new range of the codeword stream).  Returns (weights, history)."""
+    step a new range of the codeword stream).  With val_cw > 0 the mean BCE
+    on a fixed validation batch (its own seed) is evaluated every val_every
+    steps and the best weights seen are returned.  Returns (weights, history)
+    where history holds the training losses and the validation points."""
     import torch
 
     import sogrand_b200 as sg
 
     alpha = torch.full((3 * imax,), init, dtype=torch.float64, device=device, requires_grad=True)
     opt = torch.optim.Adam([alpha], lr=lr)
-    hist = []
+    hist = {"train": [], "val": []}
+    best = (float("inf"), alpha.detach().cpu().numpy().copy())
+    if val_cw:
+        vinfo, vllr = sg.gen_llr(seed + 7919, 0, val_cw, ebn0_db=ebn0_db, device=device)
+        vcb = code_bits_for(vinfo, device)
+
+    def validate(step):
+        nonlocal best
+        with torch.no_grad():
+            v = float(decode_bce(alpha.detach(), vllr, vcb, imax).item())
+        hist["val"].append((step, v))
+        if v < best[0]:
+            best = (v, alpha.detach().cpu().numpy().copy())
+        if log:
+            log(step, float("nan"), v)
+
+    if val_cw:
+        validate(0)
     for step in range(steps):
         info, llr = sg.gen_llr(seed, step * batch, batch, ebn0_db=ebn0_db, device=device)
         cb = code_bits_for(info, device)
@@ -160,7 +181,11 @@ def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax
         opt.step()
         with torch.no_grad():
             alpha.clamp_(0.0, 2.0)
-        hist.append(float(loss.item()))
+        hist["train"].append(float(loss.item()))
         if log:
-            log(step, hist[-1])
+            log(step, hist["train"][-1], None)
+        if val_cw and (step + 1) % val_every == 0:
+            validate(step + 1)
+    if val_cw:
+        return best[1], hist
     return alpha.detach().cpu().numpy(), hist

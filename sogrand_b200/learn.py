@@ -72,6 +72,8 @@ def main():
     ap.add_argument("--imax-train", type=int, default=30)
     ap.add_argument("--lr", type=float, default=0.02)
     ap.add_argument("--weights", default=None, help="json with learned weights (skip training)")
+    ap.add_argument("--val-cw", type=int, default=0, help="validation codewords (keep the best weights)")
+    ap.add_argument("--val-every", type=int, default=10)
     ap.add_argument("--eval-ebn0", default="1.25,1.5,1.75,2.0")
     ap.add_argument("--eval-cw", type=int, default=500000)
     ap.add_argument("--eval-imax", default="5,10,30")
@@ -87,21 +89,26 @@ def main():
         hist = []
     else:
         alpha, hist = diff.train_weights(steps=args.steps, batch=args.batch, ebn0_db=args.train_ebn0,
-                                         imax=args.imax_train, lr=args.lr, seed=args.seed,
-                                         log=lambda s, l: print(f"step {s} loss {l:.4f}", flush=True))
+                                         imax=args.imax_train, lr=args.lr, seed=args.seed, val_cw=args.val_cw,
+                                         val_every=args.val_every,
+                                         log=lambda s, l, v: print(f"step {s} loss {l:.4f} val {v}", flush=True))
     train_s = time.perf_counter() - t0
     res = {"weights": [float(x) for x in alpha], "train": {"steps": args.steps, "batch": args.batch,
+                                                          "val_cw": args.val_cw,
                                                           "ebn0_db": args.train_ebn0, "imax": args.imax_train,
                                                           "lr": args.lr, "loss": hist, "seconds": train_s},
            "eval": []}
     eval_seed = args.seed + 1  # a stream disjoint from training
     for eb in [float(x) for x in args.eval_ebn0.split(",")]:
         plain = evaluate(None, 30, eb, args.eval_cw, eval_seed, 0)
-        row = {"ebn0_db": eb, "plain_imax30": plain, "learned": []}
+        row = {"ebn0_db": eb, "plain_imax30": plain, "learned": [], "plain": []}
         for im in [int(x) for x in args.eval_imax.split(",")]:
             r = evaluate(alpha, im, eb, args.eval_cw, eval_seed, 0)
-            r["ber_minus_plain"] = ber_difference(r, plain)
+            r["ber_minus_plain_imax30"] = ber_difference(r, plain)
+            pl = plain if im == 30 else evaluate(None, im, eb, args.eval_cw, eval_seed, 0)
+            r["ber_minus_plain_same_imax"] = ber_difference(r, pl)
             row["learned"].append(r)
+            row["plain"].append(pl)
         res["eval"].append(row)
         print(json.dumps(row), flush=True)
     if args.out:

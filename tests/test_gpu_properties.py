@@ -120,3 +120,25 @@ def test_cli_drop_in(cuda, sg, tmp_path):
     assert out[2] == "Average NG per block: %.2f" % (st["ng"].sum() / 6)
     assert out[4] == "Average NG_p per block: %.2f" % (st["ng_p"].sum() / 6)
     assert out[-1].startswith("Throughput: ")
+
+
+def test_guess_ceiling_bounds_the_decoder(cuda, sg):
+    """The per-guess arithmetic ceiling is positive and above the decoder's
+    own guess rate on the same GPU."""
+    import ctypes as C
+    import time
+
+    from sogrand_b200 import _lib
+
+    torch = cuda
+    lib = _lib.load()
+    ceil = C.c_double()
+    assert lib.sg_guess_ceiling(2000, C.byref(ceil)) == 0
+    _, llr = sg.gen_llr(99, 0, 4096, ebn0_db=2.0, device="cuda")
+    sg.decode(llr)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, raw, _ = sg.decode(llr)
+    torch.cuda.synchronize()
+    rate = sg.stats_from_device(raw)["ng"].sum() / (time.perf_counter() - t0)
+    assert ceil.value > rate > 0
