@@ -45,6 +45,11 @@
 
 #define SG_FULL 0xffffffffu
 
+template <bool B>
+struct SgBoolTag {
+    static constexpr bool value = B;
+};
+
 struct SgLineParams {
     int32_t L;
     uint32_t tmax;     /* Tmax clamped to 2^32-1 (T never exceeds 65536) */
@@ -394,7 +399,18 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 #pragma unroll
     for (int r = 0; r < (ADJ ? 16 : 1); r++)
         adj_r[r] = 0.0;
+    /* The loop is instantiated twice.  Without a Tmax cut (TM false) every
+     * step holds 32 * G valid patterns: SG_ENUM_LEN is a multiple of 32 * G,
+     * so a step either lies inside the order table or starts at its end,
+     * where the line decode ends with T = SG_ENUM_LEN. */
+    auto guess_loop = [&](auto tm_tag) {
+    constexpr bool TM = decltype(tm_tag)::value;
+    static_assert(SG_ENUM_LEN % (32u * G) == 0, "steps tile the order table");
     for (uint32_t base = 0; !done; base += 32u * G) {
+        if (!TM && base >= SG_ENUM_LEN) {
+            T = SG_ENUM_LEN;
+            break;
+        }
         /* G patterns per lane: lane j of half h tests pattern base + 32h + j */
         uint32_t ent[G];
         double e[G];
@@ -405,10 +421,15 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         for (int h = 0; h < G; h++) {
             const uint32_t bh = base + 32u * h;
             const uint32_t t = bh + lane;
-            ent[h] = __ldg(tab + (t < SG_ENUM_LEN ? t : SG_ENUM_LEN - 1u));
-            nv[h] = bh >= SG_ENUM_LEN ? 0 : (bh + 32u <= SG_ENUM_LEN ? 32 : (int)(SG_ENUM_LEN - bh));
+            if (TM) {
+                ent[h] = __ldg(tab + (t < SG_ENUM_LEN ? t : SG_ENUM_LEN - 1u));
+                nv[h] = bh >= SG_ENUM_LEN ? 0 : (bh + 32u <= SG_ENUM_LEN ? 32 : (int)(SG_ENUM_LEN - bh));
+            } else {
+                ent[h] = __ldg(tab + t);
+                nv[h] = 32;
+            }
         }
-        if (has_tmax) {
+        if (TM) {
             /* T < Tmax is checked before each new logistic weight (:652); a cut
              * in one half ends the step there */
             bool cut_seen = false;
@@ -505,6 +526,11 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             }
         }
     }
+    };
+    if (has_tmax)
+        guess_loop(SgBoolTag<true>());
+    else
+        guess_loop(SgBoolTag<false>());
     if (ADJ) {
         /* sums over the warp; lane r keeps sorted position r */
         for (int off = 16; off > 0; off >>= 1)
