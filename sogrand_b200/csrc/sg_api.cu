@@ -1018,7 +1018,8 @@ size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
     std::vector<uint32_t> t(SG_ENUM_LEN);
     const size_t n = sg_enum_build(ic, t.data());
     const size_t m = n < cap ? n : cap;
-    memcpy(out, t.data(), m * sizeof(uint32_t));
+    for (size_t i = 0; i < m; i++)
+        out[i] = t[i] & SG_ENUM_PATTERN_MASK;
     return m;
 }
 

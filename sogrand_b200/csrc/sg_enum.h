@@ -13,6 +13,13 @@
  *   bits 0..15   the pattern over sorted positions (bit r = position r)
  *   bit 16       SG_ENUM_GS: first pattern of a new logistic weight; the
  *                reference checks T < Tmax before such a pattern (:652)
+ *   bits 17..23  8 * (1 + j) for the lowest set position 8 + j of the high
+ *                byte, 0 if the high byte is empty
+ *   bits 24..30  the same for the second-lowest set high position
+ *   bit 31       SG_ENUM_HI3: the high byte has three or more set positions
+ * Bits 17..31 are derived from bits 0..15; they are byte offsets into a
+ * per-line table of path-metric increments whose entry 0 is zero, so the
+ * decoder adds the first two high-position increments without a loop.
  * For IC >= SG_ENUM_IC_CANON the weight ranges of different Hamming weights
  * no longer interleave and the table is identical for every IC; the decoder
  * uses table SG_ENUM_IC_CANON for all of them (checked by
@@ -26,6 +33,8 @@
 
 #define SG_ENUM_LEN 65536u
 #define SG_ENUM_GS 0x10000u
+#define SG_ENUM_HI3 0x80000000u
+#define SG_ENUM_PATTERN_MASK 0x1ffffu /* bits 0..16: the exported order */
 #define SG_ENUM_IC_CANON 56
 #define SG_ENUM_NTAB (SG_ENUM_IC_CANON + 1)
 
@@ -63,6 +72,27 @@ SG_HD bool sg_enum_fill(int32_t* u, int32_t k, int32_t w, int32_t W1, int32_t n1
     return true;
 }
 
+/* Entry of pattern m (bits 0..15) with flag bits: adds bits 17..31. */
+SG_HD uint32_t sg_enum_entry(uint32_t m, uint32_t flag)
+{
+    uint32_t hi = (m >> 8) & 0xffu, o1 = 0, o2 = 0;
+    if (hi) {
+        int j = 0;
+        while (!((hi >> j) & 1u))
+            j++;
+        o1 = 8u * (uint32_t)(1 + j);
+        hi &= hi - 1u;
+    }
+    if (hi) {
+        int j = 0;
+        while (!((hi >> j) & 1u))
+            j++;
+        o2 = 8u * (uint32_t)(1 + j);
+        hi &= hi - 1u;
+    }
+    return m | flag | (o1 << 17) | (o2 << 24) | (hi ? SG_ENUM_HI3 : 0u);
+}
+
 /* The builder itself, usable on host and device (same source, same order). */
 SG_HD size_t sg_enum_build_impl(int32_t ic, uint32_t* out)
 {
@@ -87,7 +117,7 @@ SG_HD size_t sg_enum_build_impl(int32_t ic, uint32_t* out)
             if (n1 == 0) { /* the all-ones pattern; the reference divides by zero here */
                 if (t >= SG_ENUM_LEN)
                     return 0;
-                out[t++] = 0xffffu | flag;
+                out[t++] = sg_enum_entry(0xffffu, flag);
                 flag = 0;
                 continue;
             }
@@ -101,7 +131,7 @@ SG_HD size_t sg_enum_build_impl(int32_t ic, uint32_t* out)
                 uint32_t m = 0;
                 for (int32_t i = 0; i < w; i++)
                     m |= 1u << (i + u[i]);
-                out[t++] = m | flag;
+                out[t++] = sg_enum_entry(m, flag);
                 flag = 0;
                 /* landslide (:689-734): move the highest position that is at
                  * least 2 below the top one place up and refill above it */

@@ -59,7 +59,9 @@ struct SgLineParams {
 /* Per-warp shared scratch of one line decode. */
 struct SgWarpScratch {
     double A[256];      /* PM prefix over the low byte of a pattern */
-    double dhi[8];      /* PM increments of sorted positions 8..15 */
+    double dz[16];      /* dz[0] = 0, dz[1 + j] = PM increment of sorted
+                           position 8 + j (j < 8), the rest 0; indexed by the
+                           byte offsets of an order-table entry */
     double qa[16];      /* values for the tie-exact sort */
     int32_t perm[16];   /* sorted rank -> position */
     int32_t rank[16];   /* position -> sorted rank */
@@ -376,8 +378,9 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             ws->synlo[lane + 32 * i] = (uint8_t)x;
             ws->synhi[lane + 32 * i] = (uint8_t)y;
         }
-        if (lane >= 8 && lane < 16)
-            ws->dhi[lane - 8] = dl;
+        const double dsh = __shfl_sync(SG_FULL, dl, (lane + 7) & 31);
+        if (lane < 16)
+            ws->dz[lane] = (lane >= 1 && lane <= 8) ? dsh : 0.0;
     }
     __syncwarp();
 
@@ -449,12 +452,22 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 #pragma unroll
         for (int h = 0; h < G; h++) {
             const uint32_t lo = ent[h] & 0xffu;
-            uint32_t hi = (ent[h] >> 8) & 0xffu;
+            const uint32_t hi = (ent[h] >> 8) & 0xffu;
             double pm = ws->A[lo];
             const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
-            while (hi) {
-                pm = __dadd_rn(pm, ws->dhi[__ffs(hi) - 1]);
-                hi &= hi - 1u;
+            /* high positions in ascending order: the first two from the
+             * entry's offsets (offset 0 reads dz[0] = 0, and pm + 0 = pm
+             * since pm >= +0), any further ones in a loop few steps enter */
+            const char* dzb = reinterpret_cast<const char*>(ws->dz);
+            pm = __dadd_rn(pm, *reinterpret_cast<const double*>(dzb + ((ent[h] >> 17) & 0x7fu)));
+            pm = __dadd_rn(pm, *reinterpret_cast<const double*>(dzb + ((ent[h] >> 24) & 0x7fu)));
+            if (__any_sync(SG_FULL, (ent[h] & SG_ENUM_HI3) != 0u)) {
+                uint32_t rest = hi & (hi - 1u);
+                rest &= rest - 1u;
+                while (rest) {
+                    pm = __dadd_rn(pm, ws->dz[__ffs(rest)]);
+                    rest &= rest - 1u;
+                }
             }
             e[h] = sg_exp_neg(-pm, etab);
             hits[h] = __ballot_sync(SG_FULL, syn == 0u) & (nv[h] >= 32 ? SG_FULL : ((1u << nv[h]) - 1u));
