@@ -57,16 +57,25 @@ struct SgLineParams {
 };
 
 /* Per-warp shared scratch of one line decode. */
-struct SgWarpScratch {
+#define SG_LIST_MAX 8 /* SG_MAX_L of the C ABI; the entry points reject larger L */
+
+struct alignas(16) SgWarpScratch { /* A is read as double2 */
     double A[256];      /* PM prefix over the low byte of a pattern */
     double dz[16];      /* dz[0] = 0, dz[1 + j] = PM increment of sorted
                            position 8 + j (j < 8), the rest 0; indexed by the
                            byte offsets of an order-table entry */
-    double qa[16];      /* values for the tie-exact sort */
+    double qa[16];      /* values for the tie-exact sort, then the input LLRs */
     int32_t perm[16];   /* sorted rank -> position */
     int32_t rank[16];   /* position -> sorted rank */
     uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision) */
     uint8_t synhi[256]; /* syndrome of the high byte */
+    /* the list (touched only at codewords and in the soft output, so it
+     * lives here rather than in registers): entry k = exp(-PM) of the k-th
+     * codeword found and its bits (bit i = position i) */
+    double lst_e[SG_LIST_MAX];
+    uint32_t lst_cm[SG_LIST_MAX];
+    double pnl;         /* pNL of the last getLConf */
+    int32_t curl;       /* codewords listed */
 };
 
 __constant__ uint8_t c_hcol[16];
@@ -140,38 +149,32 @@ struct SgLineResult {
     int32_t ncw;      /* codewords found (all lanes) */
 };
 
-/* List state of a line decode.  Lane k < L holds entry k of the list:
- * my_e = exp(-PM) of the k-th codeword found, my_cm its bits (bit i =
- * position i).  curl and pnl are warp-uniform. */
-struct SgListState {
-    double pnl;     /* pNL of the last getLConf */
-    double my_e;
-    uint32_t my_cm;
-    int32_t curl;   /* codewords listed */
-};
-
 /* A codeword found at pattern mask `mj` (sorted positions) whose guess left
  * P_notGuess = P and contributed ej = exp(-PM): list insertion and getLConf
  * (:674-686, :767-774).  myrank: sorted rank of this lane's position (lanes
  * 0..15).  Returns true when the line decode stops. */
-__device__ __forceinline__ bool sg_list_hit(SgListState& st, const SgLineParams& lp, uint32_t hdm, uint32_t mj,
+__device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, const SgLineParams& lp, uint32_t hdm, uint32_t mj,
                                             double P, double ej, int lane, int myrank)
 {
     /* AddTEP (:761): position i flips when its sorted rank is in the pattern */
     const uint32_t cm = hdm ^ (__ballot_sync(SG_FULL, lane < 16 && ((mj >> myrank) & 1u)) & 0xffffu);
-    if (lane == st.curl) {
-        st.my_e = ej;
-        st.my_cm = cm;
-    }
+    const int curl = ws->curl;
     double ppos = 0.0;
-    for (int i = 0; i <= st.curl; i++)
-        ppos = __dadd_rn(ppos, __shfl_sync(SG_FULL, st.my_e, i));
+    for (int i = 0; i < curl; i++)
+        ppos = __dadd_rn(ppos, ws->lst_e[i]);
+    ppos = __dadd_rn(ppos, ej);
     const double pneg = __dmul_rn(0x1p-8, P); /* 2^-(n-k) * P_notGuess */
-    st.pnl = pneg;
+    __syncwarp();
+    if (lane == 0) {
+        ws->lst_e[curl] = ej;
+        ws->lst_cm[curl] = cm;
+        ws->pnl = pneg;
+        ws->curl = curl + 1;
+    }
+    __syncwarp();
     const double den = __dadd_rn(ppos, pneg);
     const double conf = (den > 1e-40) ? __ddiv_rn(ppos, den) : 1.0;
-    st.curl++;
-    return conf > lp.thres || st.curl == lp.L;
+    return conf > lp.thres || curl + 1 == lp.L;
 }
 
 /* Advance P_notGuess over lanes [0, nv) of one 32-pattern half (first pattern
@@ -181,7 +184,7 @@ __device__ __forceinline__ bool sg_list_hit(SgListState& st, const SgLineParams&
  * alone, and the scan restarts after it.  Sets T and done when the line
  * decode stops. */
 __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_t hits, int nv, uint32_t bh,
-                                                 double& P, SgListState& st, uint32_t& T, bool& done,
+                                                 double& P, SgWarpScratch* ws, uint32_t& T, bool& done,
                                                  const SgLineParams& lp, uint32_t hdm, int lane, int myrank)
 {
     int s = 0;
@@ -191,7 +194,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             P = __dsub_rn(P, es);
             if ((hits >> s) & 1u) {
                 const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
-                if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
+                if (sg_list_hit(ws, lp, hdm, mj, P, es, lane, myrank)) {
                     T = bh + (uint32_t)s + 1u;
                     done = true;
                 }
@@ -226,7 +229,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
             const double eh = __shfl_sync(SG_FULL, e, h);
             const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
-            if (sg_list_hit(st, lp, hdm, mj, Ph, eh, lane, myrank)) {
+            if (sg_list_hit(ws, lp, hdm, mj, Ph, eh, lane, myrank)) {
                 T = bh + (uint32_t)h + 1u;
                 done = true;
                 break;
@@ -242,7 +245,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             P = __dsub_rn(P, es);
             if ((hits >> f) & 1u) {
                 const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
-                if (sg_list_hit(st, lp, hdm, mj, P, es, lane, myrank)) {
+                if (sg_list_hit(ws, lp, hdm, mj, P, es, lane, myrank)) {
                     T = bh + (uint32_t)f + 1u;
                     done = true;
                 }
@@ -291,13 +294,20 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     const double jl = sg_jaclog(act ? -a_all : a_all, etab, ltab);
     const double jn = act ? jl : 0.0;
 
-    /* QuickSort of |L| ascending (:618) */
+    /* QuickSort of |L| ascending (:618): rank of each position.  Lane p and
+     * lane p + 16 count for position p the smaller (and equal) magnitudes
+     * among positions 0..7 and 8..15 respectively, then add. */
     int lt = 0, eq = 0;
+    {
+        const int p = lane & 15, j0 = lane & 16 ? 8 : 0;
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-        const double aj = __shfl_sync(SG_FULL, a, j);
-        lt += (aj < a);
-        eq += (aj == a) && (j != lane);
+        for (int k = 0; k < 8; k++) {
+            const double aj = __shfl_sync(SG_FULL, a, j0 + k);
+            lt += (aj < a_all);
+            eq += (aj == a_all) && (j0 + k != p);
+        }
+        lt += __shfl_xor_sync(SG_FULL, lt, 16);
+        eq += __shfl_xor_sync(SG_FULL, eq, 16);
     }
     /* ties (and NaN, which no comparison orders) take the exact quicksort */
     if (!__any_sync(SG_FULL, act && (eq > 0 || a != a))) {
@@ -312,10 +322,18 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         if (lane == 0)
             sg_quicksort16(ws->qa, ws->perm);
     }
+    /* getPM_HD: the JacLog terms summed in position order; A[0..15] is free
+     * until the tables below are built */
+    if (act)
+        ws->A[lane] = jn;
+    __syncwarp();
     double pmhd = 0.0;
 #pragma unroll
-    for (int i = 0; i < 16; i++)
-        pmhd = __dadd_rn(pmhd, __shfl_sync(SG_FULL, jn, i));
+    for (int i = 0; i < 8; i++) {
+        const double2 v = reinterpret_cast<const double2*>(ws->A)[i];
+        pmhd = __dadd_rn(pmhd, v.x);
+        pmhd = __dadd_rn(pmhd, v.y);
+    }
     __syncwarp();
     const int src = act ? ws->perm[lane] : 0;
     if (act)
@@ -382,8 +400,13 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         if (lane < 16)
             ws->dz[lane] = (lane >= 1 && lane <= 8) ? dsh : 0.0;
     }
-    __syncwarp();
-
+    /* the sort is done with qa: it keeps the input LLRs for the soft output */
+    if (act)
+        ws->qa[lane] = llr;
+    if (lane == 0) {
+        ws->curl = 0;
+        ws->pnl = 0.0;
+    }
     __syncwarp();
     const int myrank = act ? ws->rank[lane] : 0;
 
@@ -391,11 +414,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     const uint32_t* tab = enum_tabs + (size_t)itab * SG_ENUM_LEN;
     const bool has_tmax = lp.tmax < SG_ENUM_LEN;
     double P = 1.0; /* P_notGuess */
-    SgListState st;
-    st.pnl = 0.0;
-    st.my_e = 0.0;
-    st.my_cm = 0u;
-    st.curl = 0;
+
     uint32_t T = 0;
     bool done = false;
     double adj_tot = 0.0, adj_r[ADJ ? 16 : 1];
@@ -514,7 +533,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             for (int h = 0; h < G; h++) {
                 if (done)
                     break;
-                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, st, T, done, lp, hdm, lane,
+                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, ws, T, done, lp, hdm, lane,
                                  myrank);
                 if (!done && nv[h] < 32) {
                     T = base + 32u * h + (uint32_t)nv[h];
@@ -559,36 +578,39 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         }
         adj->etot = adj_tot;
         adj->esort = mine_r;
-        adj->pnl = st.pnl;
-        adj->my_e = st.my_e;
-        adj->my_cm = st.my_cm;
+        const int curl = ws->curl;
+        adj->pnl = ws->pnl;
+        adj->my_e = lane < curl ? ws->lst_e[lane] : 0.0;
+        adj->my_cm = lane < curl ? ws->lst_cm[lane] : 0u;
         adj->hdm = hdm;
-        adj->curl = st.curl;
+        adj->curl = curl;
         adj->myrank = myrank;
     }
 
     /* Soft output (:536-577) */
     SgLineResult res;
     res.T = T;
-    res.ncw = st.curl;
+    const int curl = ws->curl;
+    res.ncw = curl;
+    /* the input LLR of position lane & 15, kept in qa during the loop */
+    const double x = ws->qa[lane & 15];
     double lapp, le;
-    if (st.curl == 0) {
-        lapp = llr;
+    if (curl == 0) {
+        lapp = x;
         le = 0.0;
     } else {
         /* every lane works on position lane & 15; lanes 0..15 then take
          * log(p0), lanes 16..31 log(p1) */
         const int pos = lane & 15;
-        const double x = __shfl_sync(SG_FULL, llr, pos);
-        const double pnlc = fmax(st.pnl, 1e-40);
+        const double pnlc = fmax(ws->pnl, 1e-40);
         double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, sg_exp(x, etab)));
         double pp0 = __dsub_rn(1.0, pp1);
         pp1 = fmin(fmax(pp1, 1e-40), 1.0);
         pp0 = fmin(fmax(pp0, 1e-40), 1.0);
         double p1 = 0.0, p0 = 0.0;
-        for (int j = 0; j < st.curl; j++) {
-            const double c = (double)((__shfl_sync(SG_FULL, st.my_cm, j) >> pos) & 1u);
-            const double pj = __shfl_sync(SG_FULL, st.my_e, j);
+        for (int j = 0; j < curl; j++) {
+            const double c = (double)((ws->lst_cm[j] >> pos) & 1u);
+            const double pj = ws->lst_e[j];
             p1 = __dadd_rn(p1, __dmul_rn(c, pj));
             p0 = __dadd_rn(p0, __dmul_rn(__dsub_rn(1.0, c), pj));
         }
@@ -596,7 +618,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         p1 = __dadd_rn(p1, __dmul_rn(pnlc, pp1));
         const double lg = sg_log(fmax(act ? p0 : p1, 1e-40), ltab);
         lapp = __dsub_rn(lg, __shfl_sync(SG_FULL, lg, (lane & 15) + 16));
-        le = __dsub_rn(lapp, llr);
+        le = __dsub_rn(lapp, x);
     }
     res.lapp = lapp;
     res.le = le;
