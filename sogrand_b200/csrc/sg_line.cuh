@@ -76,6 +76,7 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
     uint32_t lst_cm[SG_LIST_MAX];
     double pnl;         /* pNL of the last getLConf */
     int32_t curl;       /* codewords listed */
+    uint32_t hdm;       /* hard decision, bit i = position i */
 };
 
 __constant__ uint8_t c_hcol[16];
@@ -151,13 +152,13 @@ struct SgLineResult {
 
 /* A codeword found at pattern mask `mj` (sorted positions) whose guess left
  * P_notGuess = P and contributed ej = exp(-PM): list insertion and getLConf
- * (:674-686, :767-774).  myrank: sorted rank of this lane's position (lanes
- * 0..15).  Returns true when the line decode stops. */
-__device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, const SgLineParams& lp, uint32_t hdm, uint32_t mj,
-                                            double P, double ej, int lane, int myrank)
+ * (:674-686, :767-774).  Returns true when the line decode stops. */
+__device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, const SgLineParams& lp, uint32_t mj, double P,
+                                            double ej, int lane)
 {
     /* AddTEP (:761): position i flips when its sorted rank is in the pattern */
-    const uint32_t cm = hdm ^ (__ballot_sync(SG_FULL, lane < 16 && ((mj >> myrank) & 1u)) & 0xffffu);
+    const int myrank = lane < 16 ? ws->rank[lane] : 0;
+    const uint32_t cm = ws->hdm ^ (__ballot_sync(SG_FULL, lane < 16 && ((mj >> myrank) & 1u)) & 0xffffu);
     const int curl = ws->curl;
     double ppos = 0.0;
     for (int i = 0; i < curl; i++)
@@ -185,7 +186,7 @@ __device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, const SgLineParam
  * decode stops. */
 __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_t hits, int nv, uint32_t bh,
                                                  double& P, SgWarpScratch* ws, uint32_t& T, bool& done,
-                                                 const SgLineParams& lp, uint32_t hdm, int lane, int myrank)
+                                                 const SgLineParams& lp, int lane)
 {
     int s = 0;
     while (s < nv && !done) {
@@ -194,7 +195,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             P = __dsub_rn(P, es);
             if ((hits >> s) & 1u) {
                 const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
-                if (sg_list_hit(ws, lp, hdm, mj, P, es, lane, myrank)) {
+                if (sg_list_hit(ws, lp, mj, P, es, lane)) {
                     T = bh + (uint32_t)s + 1u;
                     done = true;
                 }
@@ -229,7 +230,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
             const double eh = __shfl_sync(SG_FULL, e, h);
             const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
-            if (sg_list_hit(ws, lp, hdm, mj, Ph, eh, lane, myrank)) {
+            if (sg_list_hit(ws, lp, mj, Ph, eh, lane)) {
                 T = bh + (uint32_t)h + 1u;
                 done = true;
                 break;
@@ -245,7 +246,7 @@ __device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_
             P = __dsub_rn(P, es);
             if ((hits >> f) & 1u) {
                 const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
-                if (sg_list_hit(ws, lp, hdm, mj, P, es, lane, myrank)) {
+                if (sg_list_hit(ws, lp, mj, P, es, lane)) {
                     T = bh + (uint32_t)f + 1u;
                     done = true;
                 }
@@ -406,9 +407,9 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     if (lane == 0) {
         ws->curl = 0;
         ws->pnl = 0.0;
+        ws->hdm = hdm;
     }
     __syncwarp();
-    const int myrank = act ? ws->rank[lane] : 0;
 
     /* Guess loop (:624-744) */
     const uint32_t* tab = enum_tabs + (size_t)itab * SG_ENUM_LEN;
@@ -533,8 +534,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             for (int h = 0; h < G; h++) {
                 if (done)
                     break;
-                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, ws, T, done, lp, hdm, lane,
-                                 myrank);
+                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, ws, T, done, lp, lane);
                 if (!done && nv[h] < 32) {
                     T = base + 32u * h + (uint32_t)nv[h];
                     done = true;
@@ -584,7 +584,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         adj->my_cm = lane < curl ? ws->lst_cm[lane] : 0u;
         adj->hdm = hdm;
         adj->curl = curl;
-        adj->myrank = myrank;
+        adj->myrank = act ? ws->rank[lane] : 0;
     }
 
     /* Soft output (:536-577) */
