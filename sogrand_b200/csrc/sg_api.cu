@@ -683,6 +683,11 @@ int grid_for(unsigned long long n, int cap)
     return (int)(n < (unsigned long long)cap ? n : (unsigned long long)cap);
 }
 
+/* Host-buffer decode through the batched persistent decoder, defined with
+ * the batch handles below. */
+sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params* p, uint8_t* bits, double* lapp,
+                                sg_cw_stats* stats);
+
 } // namespace
 
 extern "C" {
@@ -805,70 +810,7 @@ sg_status sg_decode_host(const double* llr, size_t n_cw, const sg_params* p, uin
         return SG_OK;
     if (!llr || !bits)
         return fail(SG_ERR_ARG, "llr and bits must not be NULL");
-    /* bounded device footprint: chunks of at most 32768 codewords (1 GiB of LLRs) */
-    const size_t chunk = n_cw < 32768 ? n_cw : 32768;
-    double *dl = nullptr, *da = nullptr;
-    uint8_t* db = nullptr;
-    sg_cw_stats* dst = nullptr;
-    std::vector<sg_cw_stats> hst;
-    cudaError_t e;
-    bool any_nonfinite = false;
-    if ((e = cudaMalloc(&dl, chunk * SG_CUBE * sizeof(double))) != cudaSuccess ||
-        (e = cudaMalloc(&db, chunk * SG_INFO_BYTES)) != cudaSuccess ||
-        (e = cudaMalloc(&dst, chunk * sizeof(sg_cw_stats))) != cudaSuccess ||
-        (lapp && (e = cudaMalloc(&da, chunk * SG_CUBE * sizeof(double))) != cudaSuccess)) {
-        s = cuda_fail(e, "cudaMalloc");
-    } else {
-        hst.resize(chunk);
-        for (size_t off = 0; off < n_cw && s == SG_OK; off += chunk) {
-            const size_t n = (n_cw - off) < chunk ? (n_cw - off) : chunk;
-            if ((e = cudaMemcpy(dl, llr + off * SG_CUBE, n * SG_CUBE * sizeof(double), cudaMemcpyHostToDevice)) !=
-                cudaSuccess) {
-                s = cuda_fail(e, "cudaMemcpy H2D");
-                break;
-            }
-            if ((s = sg_decode_device(dl, n, p, db, da, dst, nullptr)) != SG_OK)
-                break;
-            if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
-                s = cuda_fail(e, "decode");
-                break;
-            }
-            if ((e = cudaMemcpy(bits + off * SG_INFO_BYTES, db, n * SG_INFO_BYTES, cudaMemcpyDeviceToHost)) !=
-                    cudaSuccess ||
-                (e = cudaMemcpy(hst.data(), dst, n * sizeof(sg_cw_stats), cudaMemcpyDeviceToHost)) != cudaSuccess ||
-                (lapp && (e = cudaMemcpy(lapp + off * SG_CUBE, da, n * SG_CUBE * sizeof(double),
-                                         cudaMemcpyDeviceToHost)) != cudaSuccess)) {
-                s = cuda_fail(e, "cudaMemcpy D2H");
-                break;
-            }
-            for (size_t i = 0; i < n; i++)
-                any_nonfinite |= hst[i].converged < 0;
-            {
-                DevCtx* c = nullptr;
-                unsigned int herr = 0;
-                if ((s = get_ctx(&c)) != SG_OK)
-                    break;
-                if ((e = cudaMemcpy(&herr, c->err, sizeof herr, cudaMemcpyDeviceToHost)) != cudaSuccess) {
-                    s = cuda_fail(e, "error flag");
-                    break;
-                }
-                if (herr) {
-                    cudaMemset(c->err, 0, sizeof herr);
-                    s = fail(SG_ERR_TIMEOUT, "a bulk copy into shared memory did not complete");
-                    break;
-                }
-            }
-            if (stats)
-                memcpy(stats + off, hst.data(), n * sizeof(sg_cw_stats));
-        }
-    }
-    cudaFree(dl);
-    cudaFree(db);
-    cudaFree(dst);
-    cudaFree(da);
-    if (s == SG_OK && any_nonfinite)
-        return fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
-    return s;
+    return decode_host_pipelined(llr, n_cw, p, bits, lapp, stats);
 }
 
 sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_params* p, size_t chunk_cw,
@@ -1231,6 +1173,97 @@ sg_status batch_enqueue(sg_batch b, const double* d_llr, size_t n_cw, const sg_p
     const int grid = (int)(n_cw < (size_t)c->sms ? n_cw : (size_t)c->sms);
     SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem, st));
     return SG_OK;
+}
+
+/* One half of the host-buffer pipeline: device buffers for one chunk, its
+ * stream and its work queue. */
+struct HostLane {
+    double* dl = nullptr;
+    double* da = nullptr;
+    uint8_t* db = nullptr;
+    sg_cw_stats* dst = nullptr;
+    cudaStream_t st = nullptr;
+    sg_batch_s b;
+    size_t off = 0, n = 0;
+};
+
+/* Chunks of at most 16384 codewords (512 MiB of LLRs) alternate between two
+ * lanes on two streams: while chunk k decodes, chunk k + 1 is copied in and
+ * queued behind it, so copies overlap decoding and the next chunk's CTAs
+ * take each SM as soon as the current chunk's CTA there runs out of work.
+ * Results are read back chunk by chunk in order. */
+sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params* p, uint8_t* bits, double* lapp,
+                                sg_cw_stats* stats)
+{
+    const size_t chunk = n_cw < 16384 ? n_cw : 16384;
+    const size_t nk = (n_cw + chunk - 1) / chunk;
+    HostLane ln[2];
+    sg_status s = SG_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    for (int i = 0; i < 2 && i < (int)nk && s == SG_OK; i++) {
+        HostLane& L = ln[i];
+        L.b.device = dev;
+        if ((e = cudaMalloc(&L.dl, chunk * SG_CUBE * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc(&L.db, chunk * SG_INFO_BYTES)) != cudaSuccess ||
+            (e = cudaMalloc(&L.dst, chunk * sizeof(sg_cw_stats))) != cudaSuccess ||
+            (lapp && (e = cudaMalloc(&L.da, chunk * SG_CUBE * sizeof(double))) != cudaSuccess) ||
+            (e = cudaMalloc(&L.b.q, sizeof(SgQueue))) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess)
+            s = cuda_fail(e, "device buffers");
+    }
+    std::vector<sg_cw_stats> hst(chunk);
+    bool any_nonfinite = false;
+    auto enqueue = [&](size_t k) -> sg_status {
+        HostLane& L = ln[k & 1];
+        L.off = k * chunk;
+        L.n = (n_cw - L.off) < chunk ? (n_cw - L.off) : chunk;
+        SG_CUDA(cudaMemcpyAsync(L.dl, llr + L.off * SG_CUBE, L.n * SG_CUBE * sizeof(double), cudaMemcpyHostToDevice,
+                                L.st));
+        return batch_enqueue(&L.b, L.dl, L.n, p, L.db, lapp ? L.da : nullptr, L.dst, L.st);
+    };
+    auto drain = [&](size_t k) -> sg_status {
+        HostLane& L = ln[k & 1];
+        SgQueue hq;
+        SG_CUDA(cudaMemcpyAsync(bits + L.off * SG_INFO_BYTES, L.db, L.n * SG_INFO_BYTES, cudaMemcpyDeviceToHost,
+                                L.st));
+        SG_CUDA(cudaMemcpyAsync(hst.data(), L.dst, L.n * sizeof(sg_cw_stats), cudaMemcpyDeviceToHost, L.st));
+        if (lapp)
+            SG_CUDA(cudaMemcpyAsync(lapp + L.off * SG_CUBE, L.da, L.n * SG_CUBE * sizeof(double),
+                                    cudaMemcpyDeviceToHost, L.st));
+        SG_CUDA(cudaMemcpyAsync(&hq, L.b.q, sizeof hq, cudaMemcpyDeviceToHost, L.st));
+        SG_CUDA(cudaStreamSynchronize(L.st));
+        if (hq.err)
+            return fail(SG_ERR_TIMEOUT, "a persistent-decoder warp gave up waiting for work");
+        for (size_t i = 0; i < L.n; i++)
+            any_nonfinite |= hst[i].converged < 0;
+        if (stats)
+            memcpy(stats + L.off, hst.data(), L.n * sizeof(sg_cw_stats));
+        return SG_OK;
+    };
+    if (s == SG_OK)
+        s = enqueue(0);
+    for (size_t k = 0; k < nk && s == SG_OK; k++) {
+        if (k + 1 < nk && (s = enqueue(k + 1)) != SG_OK)
+            break;
+        s = drain(k);
+    }
+    for (HostLane& L : ln) {
+        if (L.st) {
+            cudaStreamSynchronize(L.st);
+            cudaStreamDestroy(L.st);
+        }
+        cudaFree(L.dl);
+        cudaFree(L.db);
+        cudaFree(L.dst);
+        cudaFree(L.da);
+        cudaFree(L.b.q);
+    }
+    if (s == SG_OK && any_nonfinite)
+        return fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
+    return s;
 }
 
 } // namespace
