@@ -494,7 +494,7 @@ struct SgPVariant {
     { NAME, NW, C, sizeof(SgPersistSmem<NW, C>), (const void*)sg_persist_kernel<NW, C, G> }
 static const SgPVariant g_pvariants[] = {
     SG_PVARIANT(24, 3, 1, "p24x3"),
-    SG_PVARIANT(28, 4, 1, "p28x4"),
+    SG_PVARIANT(28, 3, 1, "p28x3"),
     SG_PVARIANT(16, 3, 1, "p16x3"),
     SG_PVARIANT(20, 4, 1, "p20x4"),
     SG_PVARIANT(32, 3, 1, "p32x3"),
@@ -508,7 +508,7 @@ constexpr bool sg_tables_aligned()
 {
     return offsetof(T, etab) % 16 == 0 && offsetof(T, ltab) % 16 == 0;
 }
-static_assert(sg_tables_aligned<SgPersistSmem<24, 3>>() && sg_tables_aligned<SgPersistSmem<28, 4>>() &&
+static_assert(sg_tables_aligned<SgPersistSmem<24, 3>>() && sg_tables_aligned<SgPersistSmem<28, 3>>() &&
                   sg_tables_aligned<SgPersistSmem<16, 3>>() && sg_tables_aligned<SgPersistSmem<20, 4>>() && sg_tables_aligned<SgPersistSmem<32, 3>>() &&
                   sg_tables_aligned<SgCwSmem<8, false>>() && sg_tables_aligned<SgCwSmem<8, true>>() &&
                   sg_tables_aligned<SgCwSmem<12, true>>() && sg_tables_aligned<SgCwSmem<16, false>>() &&
@@ -520,6 +520,12 @@ constexpr bool sg_bulk_aligned()
     return offsetof(T, lch) == 0 && offsetof(T, mbar) % 8 == 0;
 }
 static_assert(sg_bulk_aligned<SgCwSmem<8, true>>() && sg_bulk_aligned<SgCwSmem<12, true>>(), "bulk copy");
+/* every configuration fits the 227 KB of shared memory a CTA may have */
+static_assert(sizeof(SgPersistSmem<32, 3>) <= 227 * 1024 && sizeof(SgPersistSmem<28, 3>) <= 227 * 1024 &&
+                  sizeof(SgPersistSmem<24, 3>) <= 227 * 1024 && sizeof(SgPersistSmem<20, 4>) <= 227 * 1024 &&
+                  sizeof(SgPersistSmem<16, 3>) <= 227 * 1024 && sizeof(SgCwSmem<8, true>) <= 227 * 1024 &&
+                  sizeof(SgCwSmem<16, false>) <= 227 * 1024 && sizeof(SgCwSmem<12, true>) <= 227 * 1024,
+              "shared memory per CTA");
 
 /* Static device memory of the allocation-free entry point: the error flag
  * (first 256 bytes), then per-codeword statistics and bits for at most

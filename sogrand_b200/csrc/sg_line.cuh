@@ -23,15 +23,14 @@
  *  P_notGuess  the reference subtracts e of every guess in order (:626,
  *           :672, :712).  Within one binade [2^E, 2^(E+1)) every difference
  *           rounds to the grid u = 2^(E-52), so fl(P - e) = u*round(M - e/u)
- *           with M = P/u an integer: the running value is an exact integer
- *           prefix sum, computed by a warp scan (sums < 2^53 are exact in
- *           binary64).  When a step holds no codeword and no lane's term is
- *           large, ties, or leaves the binade, only the step's total is needed
- *           (a butterfly sum, exact for the same reason).  Otherwise a lane
- *           whose term is large, whose rounding is a tie, or whose result
- *           leaves the binade is subtracted alone with one IEEE subtraction,
- *           and the scan restarts after it.  The result equals the sequential
- *           loop bit for bit.
+ *           with M = P/u an integer: when a step holds no codeword and no
+ *           lane's term is large, ties, or leaves the binade, the running
+ *           value after the step is M minus the warp's exact integer sum (a
+ *           butterfly; sums < 2^53 are exact in binary64).  Every other step
+ *           replays the reference's sequence itself: the 32 terms are staged
+ *           in shared memory and every lane performs the 32 IEEE
+ *           subtractions in order.  The result equals the sequential loop bit
+ *           for bit.
  *  list     codewords are taken in lane order; getLConf (:767-774) uses the
  *           running P_notGuess at each, so T and the list match exactly.
  *  output   soft output of :536-577 on lanes 0..15.
@@ -65,6 +64,8 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
                            position 8 + j (j < 8), the rest 0; indexed by the
                            byte offsets of an order-table entry */
     double qa[16];      /* values for the tie-exact sort, then the input LLRs */
+    double es[32];      /* general case: exp(-PM) of the 32 patterns of a half */
+    double ps[32];      /* general case: P_notGuess after each of them */
     int32_t perm[16];   /* sorted rank -> position */
     int32_t rank[16];   /* position -> sorted rank */
     uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision) */
@@ -178,84 +179,56 @@ __device__ __forceinline__ bool sg_list_hit(SgWarpScratch* ws, const SgLineParam
     return conf > lp.thres || curl + 1 == lp.L;
 }
 
-/* Advance P_notGuess over lanes [0, nv) of one 32-pattern half (first pattern
- * index bh) and take its codewords in order.  Within a binade the running
- * value is an exact integer prefix sum (warp scan); a lane whose term is
- * large, whose rounding ties or whose result leaves the binade is subtracted
- * alone, and the scan restarts after it.  Sets T and done when the line
- * decode stops. */
-__device__ __forceinline__ void sg_chain_segment(double e, uint32_t ent, uint32_t hits, int nv, uint32_t bh,
-                                                 double& P, SgWarpScratch* ws, uint32_t& T, bool& done,
-                                                 const SgLineParams& lp, int lane)
+/* General case of one 32-pattern half (first pattern index bh, nv valid
+ * patterns): the reference's own sequence P -= e (:626, :672, :712), one
+ * IEEE subtraction per pattern in order, evaluated redundantly by every lane
+ * from the terms staged in shared memory.  Exact whatever the step holds
+ * (codewords, binade crossings, ties, large or tiny terms).  Terms of lanes
+ * >= nv are finite and subtracted too: nv < 32 only when the line decode
+ * ends in this half, after which P is not read.  With codewords in the half
+ * P is recorded after every term, then the codewords are listed in order
+ * with the P that followed each.  Sets T and done when the decode stops. */
+__device__ __forceinline__ void sg_seq_half(double e, uint32_t ent, uint32_t hits, uint32_t bh, double& P,
+                                            SgWarpScratch* ws, uint32_t& T, bool& done, const SgLineParams& lp,
+                                            int lane)
 {
-    int s = 0;
-    while (s < nv && !done) {
-        if (!(P >= 0x1p-970)) { /* zero, negative, tiny or NaN: one lane alone */
-            const double es = __shfl_sync(SG_FULL, e, s);
-            P = __dsub_rn(P, es);
-            if ((hits >> s) & 1u) {
-                const uint32_t mj = __shfl_sync(SG_FULL, ent, s) & 0xffffu;
-                if (sg_list_hit(ws, lp, mj, P, es, lane)) {
-                    T = bh + (uint32_t)s + 1u;
-                    done = true;
-                }
-            }
-            s++;
-            continue;
-        }
-        const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
-        const double u = sg_from_bits((uint64_t)(E - 52 + 1023) << 52);
-        const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
-        const double M0 = __dmul_rn(P, iu);
-        const bool mine = lane >= s && lane < nv;
-        const double q = mine ? __dmul_rn(e, iu) : 0.0;
-        const bool big = !(q < 0x1p52);
-        double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52); /* round(q), ties to even */
-        const bool tie = fabs(__dsub_rn(q, d)) == 0.5;
-        if (big)
-            d = 0.0;
-        double S = d;
+    ws->es[lane] = e;
+    __syncwarp();
+    const double2* e2 = reinterpret_cast<const double2*>(ws->es);
+    double p = P;
+    if (!hits) {
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const double y = __shfl_up_sync(SG_FULL, S, off);
-            if (lane >= off)
-                S = __dadd_rn(S, y);
+        for (int k = 0; k < 16; k++) {
+            const double2 v = e2[k];
+            p = __dsub_rn(p, v.x);
+            p = __dsub_rn(p, v.y);
         }
-        const double M = __dsub_rn(M0, S);
-        const uint32_t bm = __ballot_sync(SG_FULL, mine && (big || tie || !(M >= 0x1p52 + 1.0)));
-        const int f = bm ? __ffs(bm) - 1 : nv;
-        uint32_t hseg = hits & (f >= 32 ? SG_FULL : ((1u << f) - 1u)) & ~((1u << s) - 1u);
-        while (hseg) {
-            const int h = __ffs(hseg) - 1;
-            const double Ph = __dmul_rn(__shfl_sync(SG_FULL, M, h), u);
-            const double eh = __shfl_sync(SG_FULL, e, h);
-            const uint32_t mj = __shfl_sync(SG_FULL, ent, h) & 0xffffu;
-            if (sg_list_hit(ws, lp, mj, Ph, eh, lane)) {
-                T = bh + (uint32_t)h + 1u;
+        P = p;
+    } else {
+        double2* p2 = reinterpret_cast<double2*>(ws->ps);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const double2 v = e2[k];
+            const double p0 = __dsub_rn(p, v.x);
+            p = __dsub_rn(p0, v.y);
+            if (lane == 0)
+                p2[k] = make_double2(p0, p);
+        }
+        P = p;
+        __syncwarp();
+        uint32_t hm = hits;
+        while (hm) {
+            const int j = __ffs(hm) - 1;
+            const uint32_t mj = __shfl_sync(SG_FULL, ent, j) & 0xffffu;
+            if (sg_list_hit(ws, lp, mj, ws->ps[j], ws->es[j], lane)) {
+                T = bh + (uint32_t)j + 1u;
                 done = true;
                 break;
             }
-            hseg &= hseg - 1u;
-        }
-        if (done)
-            break;
-        if (f > s)
-            P = __dmul_rn(__shfl_sync(SG_FULL, M, f - 1), u);
-        if (f < nv) {
-            const double es = __shfl_sync(SG_FULL, e, f);
-            P = __dsub_rn(P, es);
-            if ((hits >> f) & 1u) {
-                const uint32_t mj = __shfl_sync(SG_FULL, ent, f) & 0xffffu;
-                if (sg_list_hit(ws, lp, mj, P, es, lane)) {
-                    T = bh + (uint32_t)f + 1u;
-                    done = true;
-                }
-            }
-            s = f + 1;
-        } else {
-            s = nv;
+            hm &= hm - 1u;
         }
     }
+    __syncwarp();
 }
 
 /* Extra results of a line decode run for the adjoint (ADJ = true): the
@@ -534,7 +507,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             for (int h = 0; h < G; h++) {
                 if (done)
                     break;
-                sg_chain_segment(e[h], ent[h], hits[h], nv[h], base + 32u * h, P, ws, T, done, lp, lane);
+                sg_seq_half(e[h], ent[h], hits[h], base + 32u * h, P, ws, T, done, lp, lane);
                 if (!done && nv[h] < 32) {
                     T = base + 32u * h + (uint32_t)nv[h];
                     done = true;
