@@ -498,6 +498,9 @@ static const SgPVariant g_pvariants[] = {
     SG_PVARIANT(16, 3, 1, "p16x3"),
     SG_PVARIANT(20, 4, 1, "p20x4"),
     SG_PVARIANT(32, 3, 1, "p32x3"),
+    SG_PVARIANT(32, 3, 2, "p32x3-g2"),
+    SG_PVARIANT(24, 3, 2, "p24x3-g2"),
+    SG_PVARIANT(28, 3, 2, "p28x3-g2"),
 };
 #define SG_NPVARIANTS ((int)(sizeof(g_pvariants) / sizeof(g_pvariants[0])))
 
@@ -602,8 +605,8 @@ struct DevCtx {
 };
 
 std::mutex g_mu;
-int g_pvariant = 4; /* p32x3: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
-int g_variant = 3; /* w16-gmem: fastest on B200 at 2 dB (sogrand_b200.autotune) */
+int g_pvariant = 5; /* p32x3-g2: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
+int g_variant = 4; /* w16-gmem-g2: fastest on B200 at 2 dB (sogrand_b200.autotune) */
 DevCtx g_ctx[64];
 std::vector<uint32_t> g_enum_host;
 sg_code_tables g_code;
