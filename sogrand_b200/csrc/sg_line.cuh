@@ -80,6 +80,14 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
     uint32_t hdm;       /* hard decision, bit i = position i */
 };
 
+/* Storage index of entry lo of the A table: the low nibble XORed with the
+ * high one.  The patterns of a step concentrate on few residues of lo mod 16
+ * (an 8-byte entry's bank pair); the XOR spreads them over more banks. */
+__device__ __forceinline__ uint32_t sg_swz(uint32_t lo)
+{
+    return lo ^ ((lo >> 4) & 15u);
+}
+
 __constant__ uint8_t c_hcol[16];
 __constant__ uint8_t c_prow[8];
 __constant__ uint8_t c_ptab[256];
@@ -353,14 +361,15 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         const double v1 = __dadd_rn(v0, d[5]);
         const double v2 = __dadd_rn(v0, d[6]);
         const double v3 = __dadd_rn(v1, d[6]);
-        ws->A[lane] = v0;
-        ws->A[lane + 32] = v1;
-        ws->A[lane + 64] = v2;
-        ws->A[lane + 96] = v3;
-        ws->A[lane + 128] = __dadd_rn(v0, d[7]);
-        ws->A[lane + 160] = __dadd_rn(v1, d[7]);
-        ws->A[lane + 192] = __dadd_rn(v2, d[7]);
-        ws->A[lane + 224] = __dadd_rn(v3, d[7]);
+        /* entry i is stored at sg_swz(i) */
+        ws->A[sg_swz(lane)] = v0;
+        ws->A[sg_swz(lane + 32)] = v1;
+        ws->A[sg_swz(lane + 64)] = v2;
+        ws->A[sg_swz(lane + 96)] = v3;
+        ws->A[sg_swz(lane + 128)] = __dadd_rn(v0, d[7]);
+        ws->A[sg_swz(lane + 160)] = __dadd_rn(v1, d[7]);
+        ws->A[sg_swz(lane + 192)] = __dadd_rn(v2, d[7]);
+        ws->A[sg_swz(lane + 224)] = __dadd_rn(v3, d[7]);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             uint32_t x = sl, y = sh;
@@ -446,7 +455,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         for (int h = 0; h < G; h++) {
             const uint32_t lo = ent[h] & 0xffu;
             const uint32_t hi = (ent[h] >> 8) & 0xffu;
-            double pm = ws->A[lo];
+            double pm = ws->A[sg_swz(lo)];
             const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
             /* high positions in ascending order: the first two from the
              * entry's offsets (offset 0 reads dz[0] = 0, and pm + 0 = pm
