@@ -25,12 +25,12 @@
  *           rounds to the grid u = 2^(E-52), so fl(P - e) = u*round(M - e/u)
  *           with M = P/u an integer: when a step holds no codeword and no
  *           lane's term is large, ties, or leaves the binade, the running
- *           value after the step is M minus the warp's exact integer sum (a
- *           butterfly; sums < 2^53 are exact in binary64).  Every other step
- *           replays the reference's sequence itself: the 32 terms are staged
- *           in shared memory and every lane performs the 32 IEEE
- *           subtractions in order.  The result equals the sequential loop bit
- *           for bit.
+ *           value after the step is M minus the warp's exact integer sum
+ *           (two 32-bit warp reductions of the terms' 26-bit halves).
+ *           Every other step replays the reference's sequence itself: the
+ *           32 terms are staged in shared memory and every lane performs the
+ *           32 IEEE subtractions in order.  The result equals the sequential
+ *           loop bit for bit.
  *  list     codewords are taken in lane order; getLConf (:767-774) uses the
  *           running P_notGuess at each, so T and the list match exactly.
  *  output   soft output of :536-577 on lanes 0..15.
@@ -489,20 +489,27 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         if (!any_hit && P >= 0x1p-970) {
             const int E = (int)((sg_bits(P) >> 52) & 0x7ffu) - 1023;
             const double iu = sg_from_bits((uint64_t)(52 - E + 1023) << 52);
-            double dsum = 0.0;
+            /* d = round(q) < 2^52 is the mantissa of q + 2^52; its two 26-bit
+             * halves are summed over the warp in 32-bit integers (at most
+             * 32 * G terms below 2^26 each) */
+            static_assert(G <= 2, "32-bit sums of 26-bit halves hold 64 terms");
+            uint32_t slo = 0u, shi = 0u;
             bool bad = false;
 #pragma unroll
             for (int h = 0; h < G; h++) {
                 const double q = lane < nv[h] ? __dmul_rn(e[h], iu) : 0.0;
-                const double d = __dsub_rn(__dadd_rn(q, 0x1p52), 0x1p52);
+                const double t = __dadd_rn(q, 0x1p52);
+                const double d = __dsub_rn(t, 0x1p52);
                 bad |= !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
-                dsum = __dadd_rn(dsum, d); /* < 2^53 unless the step crosses anyway */
+                const uint64_t tb = sg_bits(t);
+                slo += (uint32_t)tb & 0x3ffffffu;
+                shi += (uint32_t)(tb >> 26) & 0x3ffffffu;
             }
             if (!__any_sync(SG_FULL, bad)) {
-                double tot = dsum;
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1)
-                    tot = __dadd_rn(tot, __shfl_xor_sync(SG_FULL, tot, off));
+                const uint32_t tlo = __reduce_add_sync(SG_FULL, slo);
+                const uint32_t thi = __reduce_add_sync(SG_FULL, shi);
+                /* exact below 2^53; a larger (rounded) total fails the test below */
+                const double tot = __dadd_rn(__dmul_rn(__uint2double_rn(thi), 0x1p26), __uint2double_rn(tlo));
                 const double M0 = __dmul_rn(P, iu);
                 if (tot <= __dsub_rn(M0, 0x1p52 + 1.0)) {
                     P = __dmul_rn(__dsub_rn(M0, tot), sg_from_bits((uint64_t)(E - 52 + 1023) << 52));
