@@ -91,6 +91,37 @@ def test_nonfinite_codeword_is_reported(cuda, sg):
         assert np.array_equal(bits[i], good_b[i]) and st[i] == good_s[i]
 
 
+def test_host_pipeline_matches_device_across_chunks(cuda, sg):
+    """sg_decode_host decodes in 16384-codeword chunks on two streams with
+    the batched decoder.  Over three chunks (the last one partial) its bits,
+    statistics and soft output equal the device entry point's (the plain
+    decoder), and a non-finite codeword in the middle chunk is reported
+    without disturbing the others."""
+    torch = cuda
+    from sogrand_b200 import _lib
+
+    n = 2 * 16384 + 1000
+    _, dllr = sg.gen_llr(77, 0, n, ebn0_db=2.5, device="cuda")
+    db, draw, dl = sg.decode(dllr, want_lapp=True)
+    torch.cuda.synchronize()
+    llr = dllr.cpu().numpy()
+    ref_bits, ref_st, ref_lapp = db.cpu().numpy(), sg.stats_from_device(draw), dl.cpu().numpy()
+    del dllr, db, draw, dl
+    bad = 20000
+    llr[bad, 5] = np.inf
+    bits = np.zeros((n, 64), np.uint8)
+    st = np.zeros(n, sg.STATS_DTYPE)
+    lapp = np.zeros((n, 4096))
+    r = _lib.load().sg_decode_host(llr.ctypes.data, n, C.byref(sg.params()), bits.ctypes.data, lapp.ctypes.data,
+                                   st.ctypes.data)
+    assert r == 3  # SG_ERR_NONFINITE, after decoding the rest
+    keep = np.arange(n) != bad
+    assert np.array_equal(bits[keep], ref_bits[keep])
+    assert np.array_equal(st[keep], ref_st[keep])
+    assert np.array_equal(lapp[keep].view(np.int64), ref_lapp[keep].view(np.int64))
+    assert st["converged"][bad] == -1 and np.all(bits[bad] == 0)
+
+
 def test_determinism_and_stats_at_scale(cuda, sg):
     torch = cuda
     n = 4096
