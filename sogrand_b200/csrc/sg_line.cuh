@@ -38,6 +38,7 @@
  * reference performs is a separately rounded IEEE operation here.
  */
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 #include "sg_enum.h"
 #include "sg_math.h"
@@ -79,6 +80,8 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
     int32_t curl;       /* codewords listed */
     uint32_t hdm;       /* hard decision, bit i = position i */
 };
+static_assert(offsetof(SgWarpScratch, synlo) % 8 == 0 && offsetof(SgWarpScratch, synhi) % 8 == 0,
+              "syndrome tables are written 8 bytes at a time");
 
 /* Storage index of entry lo of the A table: the low nibble XORed with a
  * function of bits 5..7 (their 8 values, 0, 5, 11, 14, 15, 10, 4, 1, are
@@ -343,7 +346,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     /* syndrome of the hard decision */
     const uint32_t s0 = __reduce_xor_sync(SG_FULL, (act && ((hdm >> lane) & 1u)) ? (uint32_t)c_hcol[lane] : 0u);
 
-    /* per-line tables; lane j fills entries j + 32*i, i = 0..7 */
+    /* per-line tables; lane j fills A entries j + 32*i, i = 0..7, and
+     * syndrome entries 8*j + k, k = 0..7 */
     {
         double d[8];
         uint32_t hl[8], hh[8];
@@ -359,8 +363,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         for (int b = 0; b < 5; b++)
             if ((lane >> b) & 1) {
                 v0 = __dadd_rn(v0, d[b]);
-                sl ^= hl[b];
-                sh ^= hh[b];
+                sl ^= hl[3 + b];
+                sh ^= hh[3 + b];
             }
         const double v1 = __dadd_rn(v0, d[5]);
         const double v2 = __dadd_rn(v0, d[6]);
@@ -374,15 +378,13 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         ws->A[sg_swz(lane + 160)] = __dadd_rn(v1, d[7]);
         ws->A[sg_swz(lane + 192)] = __dadd_rn(v2, d[7]);
         ws->A[sg_swz(lane + 224)] = __dadd_rn(v3, d[7]);
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            uint32_t x = sl, y = sh;
-            if (i & 1) { x ^= hl[5]; y ^= hh[5]; }
-            if (i & 2) { x ^= hl[6]; y ^= hh[6]; }
-            if (i & 4) { x ^= hl[7]; y ^= hh[7]; }
-            ws->synlo[lane + 32 * i] = (uint8_t)x;
-            ws->synhi[lane + 32 * i] = (uint8_t)y;
-        }
+        /* byte k of the 8 entries 8*lane + k: the lane's syndrome (positions
+         * 3..7) XOR those of positions 0..2 selected by k, built in place
+         * in two 32-bit words (every value is below 256) */
+        const uint32_t lo0 = sl * 0x01010101u ^ hl[0] * 0x01000100u ^ hl[1] * 0x01010000u;
+        const uint32_t hi0 = sh * 0x01010101u ^ hh[0] * 0x01000100u ^ hh[1] * 0x01010000u;
+        reinterpret_cast<uint2*>(ws->synlo)[lane] = make_uint2(lo0, lo0 ^ hl[2] * 0x01010101u);
+        reinterpret_cast<uint2*>(ws->synhi)[lane] = make_uint2(hi0, hi0 ^ hh[2] * 0x01010101u);
         const double dsh = __shfl_sync(SG_FULL, dl, (lane + 7) & 31);
         if (lane < 16)
             ws->dz[lane] = (lane >= 1 && lane <= 8) ? dsh : 0.0;
