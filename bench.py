@@ -40,6 +40,11 @@ SEED = 20260101
 EBN0 = 2.0
 # bytes per codeword the decode must move: 4096 float64 in, 64 bytes of bits out
 ALG_BYTES_PER_CW = 4096 * 8 + 64
+# DRAM bytes (read + write) per codeword of the decode kernel, from one ncu
+# capture of 2368 codewords at 2 dB (profiles/): traffic grows with the
+# codewords a launch decodes (the cubes are read once), so a full launch's
+# traffic is this times its codewords.
+DRAM_BYTES_PER_CW = {"batch": (78.752e6 + 2.577e6) / 2368, "plain": (78.98e6 + 1.63e6) / 2368}
 
 
 def dist_env():
@@ -337,7 +342,9 @@ def main():
                               "how": "sg_guess_ceiling: PM add + exp(-PM) + P_notGuess subtract per guess, "
                                      "all SMs, measured on this GPU in this run"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None,
+                         "frac": achieved / hbm_peak, "traffic": DRAM_BYTES_PER_CW[args.form] * n,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of 2368 codewords "
+                                           "(profiles/), scaled to this launch's codewords",
                          "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},
             "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
             "form": args.form, "autotune": tune,
