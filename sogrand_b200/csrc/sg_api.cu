@@ -970,7 +970,7 @@ size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
     const size_t n = sg_enum_build(ic, t.data());
     const size_t m = n < cap ? n : cap;
     for (size_t i = 0; i < m; i++)
-        out[i] = t[i] & SG_ENUM_PATTERN_MASK;
+        out[i] = sg_ent_pattern(t[i]) | (t[i] & SG_ENUM_GS);
     return m;
 }
 

@@ -60,7 +60,8 @@ struct SgLineParams {
 #define SG_LIST_MAX 8 /* SG_MAX_L of the C ABI; the entry points reject larger L */
 
 struct alignas(16) SgWarpScratch { /* A is read as double2 */
-    double A[256];      /* PM prefix over the low byte of a pattern */
+    double A[256];      /* PM prefix over the low byte of a pattern, entry lo
+                           stored at sg_swz(lo) */
     double dz[16];      /* dz[0] = 0, dz[1 + j] = PM increment of sorted
                            position 8 + j (j < 8), the rest 0; indexed by the
                            byte offsets of an order-table entry */
@@ -69,7 +70,8 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
     double ps[32];      /* general case: P_notGuess after each of them */
     int32_t perm[16];   /* sorted rank -> position */
     int32_t rank[16];   /* position -> sorted rank */
-    uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision) */
+    uint8_t synlo[256]; /* syndrome of the low byte (and of the hard decision),
+                           entry lo stored at sg_swz(lo) */
     uint8_t synhi[256]; /* syndrome of the high byte */
     /* the list (touched only at codewords and in the soft output, so it
      * lives here rather than in registers): entry k = exp(-PM) of the k-th
@@ -82,18 +84,6 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
 };
 static_assert(offsetof(SgWarpScratch, synlo) % 8 == 0 && offsetof(SgWarpScratch, synhi) % 8 == 0,
               "syndrome tables are written 8 bytes at a time");
-
-/* Storage index of entry lo of the A table: the low nibble XORed with a
- * function of bits 5..7 (their 8 values, 0, 5, 11, 14, 15, 10, 4, 1, are
- * the nibbles of the constant, low first).  The patterns of a step
- * concentrate on few residues of lo mod 16 (an 8-byte entry's bank pair);
- * this permutation, the best of a search over linear maps on steps of 2 dB
- * decodes, spreads them: 3.3 shared-memory wavefronts per lookup on
- * average instead of 5.3. */
-__device__ __forceinline__ uint32_t sg_swz(uint32_t lo)
-{
-    return lo ^ ((0x14AFEB50u >> ((lo >> 3) & 28u)) & 15u);
-}
 
 __constant__ uint8_t c_hcol[16];
 __constant__ uint8_t c_prow[8];
@@ -234,7 +224,7 @@ __device__ __forceinline__ void sg_seq_half(double e, uint32_t ent, uint32_t hit
         uint32_t hm = hits;
         while (hm) {
             const int j = __ffs(hm) - 1;
-            const uint32_t mj = __shfl_sync(SG_FULL, ent, j) & 0xffffu;
+            const uint32_t mj = sg_ent_pattern(__shfl_sync(SG_FULL, ent, j));
             if (sg_list_hit(ws, lp, mj, ws->ps[j], ws->es[j], lane)) {
                 T = bh + (uint32_t)j + 1u;
                 done = true;
@@ -383,7 +373,16 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
          * in two 32-bit words (every value is below 256) */
         const uint32_t lo0 = sl * 0x01010101u ^ hl[0] * 0x01000100u ^ hl[1] * 0x01010000u;
         const uint32_t hi0 = sh * 0x01010101u ^ hh[0] * 0x01000100u ^ hh[1] * 0x01010000u;
-        reinterpret_cast<uint2*>(ws->synlo)[lane] = make_uint2(lo0, lo0 ^ hl[2] * 0x01010101u);
+        {
+            /* stored at sg_swz(8*lane + k) = 8*lane' + (k ^ c): group lane' =
+             * lane ^ (g >> 3), bytes permuted by c = g & 7, g the XOR value
+             * of the group's bits 5..7 */
+            const uint32_t g = (0x14AFEB50u >> (4 * (lane >> 2))) & 15u;
+            const uint32_t lo1 = lo0 ^ hl[2] * 0x01010101u;
+            const uint32_t sel = 0x3210u ^ ((g & 3u) * 0x1111u);
+            const uint32_t w0 = __byte_perm(lo0, 0u, sel), w1 = __byte_perm(lo1, 0u, sel);
+            reinterpret_cast<uint2*>(ws->synlo)[lane ^ (g >> 3)] = (g & 4u) ? make_uint2(w1, w0) : make_uint2(w0, w1);
+        }
         reinterpret_cast<uint2*>(ws->synhi)[lane] = make_uint2(hi0, hi0 ^ hh[2] * 0x01010101u);
         const double dsh = __shfl_sync(SG_FULL, dl, (lane + 7) & 31);
         if (lane < 16)
@@ -459,9 +458,9 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         }
 #pragma unroll
         for (int h = 0; h < G; h++) {
-            const uint32_t lo = ent[h] & 0xffu;
+            const uint32_t lo = ent[h] & 0xffu; /* already the storage index sg_swz(low byte) */
             const uint32_t hi = (ent[h] >> 8) & 0xffu;
-            double pm = ws->A[sg_swz(lo)];
+            double pm = ws->A[lo];
             const uint32_t syn = (uint32_t)ws->synlo[lo] ^ (uint32_t)ws->synhi[hi];
             /* high positions in ascending order: the first two from the
              * entry's offsets (offset 0 reads dz[0] = 0, and pm + 0 = pm
@@ -544,7 +543,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             for (int h = 0; h < G; h++) {
                 if (base + 32u * h + (uint32_t)lane < T) {
                     adj_tot += e[h];
-                    const uint32_t m = ent[h] & 0xffffu;
+                    const uint32_t m = sg_ent_pattern(ent[h]);
 #pragma unroll
                     for (int r = 0; r < (ADJ ? 16 : 1); r++)
                         if ((m >> r) & 1u)
