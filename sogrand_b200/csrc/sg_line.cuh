@@ -66,6 +66,7 @@ struct alignas(16) SgWarpScratch { /* A is read as double2 */
                            position 8 + j (j < 8), the rest 0; indexed by the
                            byte offsets of an order-table entry */
     double qa[16];      /* values for the tie-exact sort, then the input LLRs */
+    double ex[16];      /* exp(input LLR) of each position, for the soft output */
     double es[32];      /* general case: exp(-PM) of the 32 patterns of a half */
     double ps[32];      /* general case: P_notGuess after each of them */
     int32_t perm[16];   /* sorted rank -> position */
@@ -270,8 +271,19 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     /* lanes 0..15: JacLog(-|L_i|); lanes 16..31: JacLog(+|L_(lane-16)|), used
      * for the sorted PM increments below */
     const double a_all = __shfl_sync(SG_FULL, a, lane & 15);
-    const double jl = sg_jaclog(act ? -a_all : a_all, etab, ltab);
+    const double xj = act ? -a_all : a_all;
+    const double ex = sg_exp(xj, etab);
+    /* sg_jaclog(xj) (:762), with its exp kept */
+    const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : sg_log(1.0 + ex, ltab));
     const double jn = act ? jl : 0.0;
+    {
+        /* the soft output's exp(LLR) of position p is this exp of lane p + 16
+         * when the LLR is positive, of lane p otherwise (a NaN LLR is its own
+         * exp) */
+        const double lp_ = __shfl_sync(SG_FULL, llr, lane & 15);
+        if (act ? !(lp_ > 0.0) : (lp_ > 0.0))
+            ws->ex[lane & 15] = lp_ == lp_ ? ex : lp_;
+    }
 
     /* QuickSort of |L| ascending (:618): rank of each position.  Lane p and
      * lane p + 16 count for position p the smaller (and equal) magnitudes
@@ -597,7 +609,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
          * log(p0), lanes 16..31 log(p1) */
         const int pos = lane & 15;
         const double pnlc = fmax(ws->pnl, 1e-40);
-        double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, sg_exp(x, etab)));
+        double pp1 = __ddiv_rn(1.0, __dadd_rn(1.0, ws->ex[pos]));
         double pp0 = __dsub_rn(1.0, pp1);
         pp1 = fmin(fmax(pp1, 1e-40), 1.0);
         pp0 = fmin(fmax(pp0, 1e-40), 1.0);
