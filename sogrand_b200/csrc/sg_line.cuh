@@ -287,18 +287,32 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
     /* QuickSort of |L| ascending (:618): rank of each position.  Lane p and
      * lane p + 16 count for position p the smaller (and equal) magnitudes
-     * among positions 0..7 and 8..15 respectively, then add. */
+     * among positions 0..7 and 8..15 respectively, then add.  The
+     * magnitudes are non-negative, so their high 32 bits order them unless
+     * two are equal there; only then are the full values compared. */
     int lt = 0, eq = 0;
     {
         const int p = lane & 15, j0 = lane & 16 ? 8 : 0;
+        const uint32_t ah = (uint32_t)(sg_bits(a) >> 32), mine = (uint32_t)(sg_bits(a_all) >> 32);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            const double aj = __shfl_sync(SG_FULL, a, j0 + k);
-            lt += (aj < a_all);
-            eq += (aj == a_all) && (j0 + k != p);
+            const uint32_t hj = __shfl_sync(SG_FULL, ah, j0 + k);
+            lt += (hj < mine);
+            eq += (hj == mine) && (j0 + k != p);
+        }
+        eq += __shfl_xor_sync(SG_FULL, eq, 16);
+        if (__any_sync(SG_FULL, act && eq > 0)) {
+            lt = 0;
+            eq = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const double aj = __shfl_sync(SG_FULL, a, j0 + k);
+                lt += (aj < a_all);
+                eq += (aj == a_all) && (j0 + k != p);
+            }
+            eq += __shfl_xor_sync(SG_FULL, eq, 16);
         }
         lt += __shfl_xor_sync(SG_FULL, lt, 16);
-        eq += __shfl_xor_sync(SG_FULL, eq, 16);
     }
     /* ties (and NaN, which no comparison orders) take the exact quicksort */
     if (!__any_sync(SG_FULL, act && (eq > 0 || a != a))) {
@@ -351,11 +365,21 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     /* per-line tables; lane j fills A entries j + 32*i, i = 0..7, and
      * syndrome entries 8*j + k, k = 0..7 */
     {
+        /* the increments by sorted rank, through es (free until the guess
+         * loop) */
+        if (act)
+            ws->es[lane] = dl;
+        __syncwarp();
         double d[8];
         uint32_t hl[8], hh[8];
 #pragma unroll
+        for (int b = 0; b < 8; b += 2) {
+            const double2 v = reinterpret_cast<const double2*>(ws->es)[b / 2];
+            d[b] = v.x;
+            d[b + 1] = v.y;
+        }
+#pragma unroll
         for (int b = 0; b < 8; b++) {
-            d[b] = __shfl_sync(SG_FULL, dl, b);
             hl[b] = __shfl_sync(SG_FULL, hs, b);
             hh[b] = __shfl_sync(SG_FULL, hs, 8 + b);
         }
@@ -396,9 +420,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             reinterpret_cast<uint2*>(ws->synlo)[lane ^ (g >> 3)] = (g & 4u) ? make_uint2(w1, w0) : make_uint2(w0, w1);
         }
         reinterpret_cast<uint2*>(ws->synhi)[lane] = make_uint2(hi0, hi0 ^ hh[2] * 0x01010101u);
-        const double dsh = __shfl_sync(SG_FULL, dl, (lane + 7) & 31);
         if (lane < 16)
-            ws->dz[lane] = (lane >= 1 && lane <= 8) ? dsh : 0.0;
+            ws->dz[lane] = (lane >= 1 && lane <= 8) ? ws->es[lane + 7] : 0.0;
     }
     /* the sort is done with qa: it keeps the input LLRs for the soft output */
     if (act)
