@@ -273,7 +273,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
     const double a_all = __shfl_sync(SG_FULL, a, lane & 15);
     const double xj = act ? -a_all : a_all;
     const double ex = sg_exp(xj, etab);
-    /* sg_jaclog(xj) (:762), with its exp kept */
+    /* JacLog(xj) = xj if xj > 50, 0 if xj < -50, else log(1 + e^xj) (:762),
+     * with its exp kept */
     const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : sg_log(1.0 + ex, ltab));
     const double jn = act ? jl : 0.0;
     {

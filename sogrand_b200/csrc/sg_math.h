@@ -211,13 +211,3 @@ SG_HD double sg_log(double x, const double* tab)
     return s2 + lo;
 }
 
-/* JacLog(x) = log(1 + e^x) with the reference's clamps
- * (SOGRAND_C/cubic_decoder_final.c:762). */
-SG_HD double sg_jaclog(double x, const double* etab, const double* ltab)
-{
-    if (x > 50)
-        return x;
-    if (x < -50)
-        return 0.0;
-    return sg_log(1.0 + sg_exp(x, etab), ltab);
-}
