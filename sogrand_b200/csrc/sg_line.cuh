@@ -299,9 +299,9 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         for (int k = 0; k < 8; k++) {
             const uint32_t hj = __shfl_sync(SG_FULL, ah, j0 + k);
             lt += (hj < mine);
-            eq += (hj == mine) && (j0 + k != p);
+            eq += (hj == mine);
         }
-        eq += __shfl_xor_sync(SG_FULL, eq, 16);
+        eq += __shfl_xor_sync(SG_FULL, eq, 16) - 1; /* less the position itself */
         if (__any_sync(SG_FULL, act && eq > 0)) {
             lt = 0;
             eq = 0;
