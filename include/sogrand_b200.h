@@ -106,11 +106,15 @@ sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
 
 /* Same with host buffers: copies in, decodes, copies out, synchronises.
  * Runs the batched persistent decoder (current sg_batch variant) over
- * chunks of at most 16384 codewords on two streams, so the copy of one
- * chunk overlaps the decode of the previous one (pinned host buffers let
- * the copies run asynchronously).  Results are bit-identical to
- * sg_decode_device.  Returns SG_ERR_NONFINITE (after decoding the rest) if
- * any codeword had a non-finite LLR; those codewords report converged = -1. */
+ * chunks of at most 16384 codewords, two in flight on two streams, so
+ * copies overlap decoding (pinned host buffers let the copies run
+ * asynchronously).  The chunk buffers, streams and queues are allocated by
+ * the first call on each device (about 1 GiB, 1 GiB more once L_APP is
+ * requested) and kept until the process exits; calls on one device are
+ * serialised.  Results
+ * are bit-identical to sg_decode_device.  Returns SG_ERR_NONFINITE (after
+ * decoding the rest) if any codeword had a non-finite LLR; those codewords
+ * report converged = -1. */
 sg_status sg_decode_host(const double* llr, size_t n_cw, const sg_params* p,
                          uint8_t* bits, double* lapp, sg_cw_stats* stats);
 

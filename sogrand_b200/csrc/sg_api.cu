@@ -1196,37 +1196,91 @@ struct HostLane {
     size_t off = 0, n = 0;
 };
 
-/* Chunks of at most 16384 codewords (512 MiB of LLRs) alternate between two
- * lanes on two streams: while chunk k decodes, chunk k + 1 is copied in and
- * queued behind it, so copies overlap decoding and the next chunk's CTAs
- * take each SM as soon as the current chunk's CTA there runs out of work.
- * Results are read back chunk by chunk in order. */
+/* Device resources of the host-buffer pipeline, kept per device across
+ * calls so that a call allocates nothing after the first: two lanes of
+ * chunk buffers, their streams and work queues.  Calls on one device are
+ * serialised by the mutex. */
+constexpr int SG_HOST_LANES = 2;
+constexpr size_t SG_HOST_CHUNK = 16384;
+struct HostPipe {
+    std::mutex mu;
+    HostLane ln[SG_HOST_LANES];
+    bool ready = false;     /* buffers (without L_APP), streams and queues */
+    bool has_lapp = false;  /* L_APP buffers too */
+};
+constexpr int SG_HOST_MAX_DEV = 64;
+HostPipe g_host_pipe[SG_HOST_MAX_DEV];
+
+sg_status host_pipe_setup(HostPipe& hp, int dev, bool want_lapp)
+{
+    cudaError_t e = cudaSuccess;
+    if (!hp.ready) {
+        for (HostLane& L : hp.ln) {
+            L.b.device = dev;
+            if ((e = cudaMalloc(&L.dl, SG_HOST_CHUNK * SG_CUBE * sizeof(double))) != cudaSuccess ||
+                (e = cudaMalloc(&L.db, SG_HOST_CHUNK * SG_INFO_BYTES)) != cudaSuccess ||
+                (e = cudaMalloc(&L.dst, SG_HOST_CHUNK * sizeof(sg_cw_stats))) != cudaSuccess ||
+                (e = cudaMalloc(&L.b.q, sizeof(SgQueue))) != cudaSuccess ||
+                (e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess)
+                break;
+        }
+        if (e != cudaSuccess) { /* undo a partial set-up; the next call retries */
+            for (HostLane& L : hp.ln) {
+                cudaFree(L.dl);
+                cudaFree(L.db);
+                cudaFree(L.dst);
+                cudaFree(L.b.q);
+                if (L.st)
+                    cudaStreamDestroy(L.st);
+                L = HostLane();
+            }
+            return cuda_fail(e, "host pipeline buffers");
+        }
+        hp.ready = true;
+    }
+    if (want_lapp && !hp.has_lapp) {
+        for (HostLane& L : hp.ln)
+            if ((e = cudaMalloc(&L.da, SG_HOST_CHUNK * SG_CUBE * sizeof(double))) != cudaSuccess)
+                break;
+        if (e != cudaSuccess) {
+            for (HostLane& L : hp.ln) {
+                cudaFree(L.da);
+                L.da = nullptr;
+            }
+            return cuda_fail(e, "host pipeline L_APP buffers");
+        }
+        hp.has_lapp = true;
+    }
+    return SG_OK;
+}
+
+/* Chunks of at most 16384 codewords (512 MiB of LLRs) alternate between the
+ * two lanes: while chunk k decodes, chunk k + 1 is copied in and queued
+ * behind it, so copies overlap decoding and the next chunk's CTAs take each
+ * SM as soon as the current chunk's CTA there runs out of work.  Results
+ * are read back chunk by chunk in order; a lane is refilled only after its
+ * chunk has been read back. */
 sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params* p, uint8_t* bits, double* lapp,
                                 sg_cw_stats* stats)
 {
-    const size_t chunk = n_cw < 16384 ? n_cw : 16384;
+    const size_t chunk = n_cw < SG_HOST_CHUNK ? n_cw : SG_HOST_CHUNK;
     const size_t nk = (n_cw + chunk - 1) / chunk;
-    HostLane ln[2];
-    sg_status s = SG_OK;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaGetDevice");
-    for (int i = 0; i < 2 && i < (int)nk && s == SG_OK; i++) {
-        HostLane& L = ln[i];
-        L.b.device = dev;
-        if ((e = cudaMalloc(&L.dl, chunk * SG_CUBE * sizeof(double))) != cudaSuccess ||
-            (e = cudaMalloc(&L.db, chunk * SG_INFO_BYTES)) != cudaSuccess ||
-            (e = cudaMalloc(&L.dst, chunk * sizeof(sg_cw_stats))) != cudaSuccess ||
-            (lapp && (e = cudaMalloc(&L.da, chunk * SG_CUBE * sizeof(double))) != cudaSuccess) ||
-            (e = cudaMalloc(&L.b.q, sizeof(SgQueue))) != cudaSuccess ||
-            (e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess)
-            s = cuda_fail(e, "device buffers");
-    }
+    if (dev < 0 || dev >= SG_HOST_MAX_DEV)
+        return fail(SG_ERR_ARG, "device index beyond the host pipeline's table");
+    HostPipe& hp = g_host_pipe[dev];
+    std::lock_guard<std::mutex> lk(hp.mu);
+    sg_status s = host_pipe_setup(hp, dev, lapp != nullptr);
+    if (s != SG_OK)
+        return s;
+    HostLane* ln = hp.ln;
     std::vector<sg_cw_stats> hst(chunk);
     bool any_nonfinite = false;
     auto enqueue = [&](size_t k) -> sg_status {
-        HostLane& L = ln[k & 1];
+        HostLane& L = ln[k % SG_HOST_LANES];
         L.off = k * chunk;
         L.n = (n_cw - L.off) < chunk ? (n_cw - L.off) : chunk;
         SG_CUDA(cudaMemcpyAsync(L.dl, llr + L.off * SG_CUBE, L.n * SG_CUBE * sizeof(double), cudaMemcpyHostToDevice,
@@ -1234,7 +1288,7 @@ sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params*
         return batch_enqueue(&L.b, L.dl, L.n, p, L.db, lapp ? L.da : nullptr, L.dst, L.st);
     };
     auto drain = [&](size_t k) -> sg_status {
-        HostLane& L = ln[k & 1];
+        HostLane& L = ln[k % SG_HOST_LANES];
         SgQueue hq;
         SG_CUDA(cudaMemcpyAsync(bits + L.off * SG_INFO_BYTES, L.db, L.n * SG_INFO_BYTES, cudaMemcpyDeviceToHost,
                                 L.st));
@@ -1252,24 +1306,17 @@ sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params*
             memcpy(stats + L.off, hst.data(), L.n * sizeof(sg_cw_stats));
         return SG_OK;
     };
-    if (s == SG_OK)
-        s = enqueue(0);
+    for (size_t k = 0; k < (size_t)SG_HOST_LANES && k < nk && s == SG_OK; k++)
+        s = enqueue(k);
     for (size_t k = 0; k < nk && s == SG_OK; k++) {
-        if (k + 1 < nk && (s = enqueue(k + 1)) != SG_OK)
+        if ((s = drain(k)) != SG_OK)
             break;
-        s = drain(k);
+        if (k + SG_HOST_LANES < nk)
+            s = enqueue(k + SG_HOST_LANES);
     }
-    for (HostLane& L : ln) {
-        if (L.st) {
-            cudaStreamSynchronize(L.st);
-            cudaStreamDestroy(L.st);
-        }
-        cudaFree(L.dl);
-        cudaFree(L.db);
-        cudaFree(L.dst);
-        cudaFree(L.da);
-        cudaFree(L.b.q);
-    }
+    /* leave no work of this call running on the lanes' streams */
+    for (HostLane& L : hp.ln)
+        cudaStreamSynchronize(L.st);
     if (s == SG_OK && any_nonfinite)
         return fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
     return s;
