@@ -117,7 +117,7 @@ struct SgBackSmem {
 };
 
 template <int NW>
-__global__ void __launch_bounds__(NW * 32, 1) sg_backward_kernel(const __grid_constant__ SgBackwardArgs args)
+__global__ void __launch_bounds__(NW * 32, 3) sg_backward_kernel(const __grid_constant__ SgBackwardArgs args)
 {
     constexpr int NT = NW * 32;
     SgBackSmem<NW>& S = *reinterpret_cast<SgBackSmem<NW>*>(sg_smem_raw);
