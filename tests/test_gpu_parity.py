@@ -8,6 +8,7 @@ differently from the kernel's (both within 1 ulp); the fixtures record those
 codewords, and the kernel must reproduce the twin there."""
 import hashlib
 import multiprocessing as mp
+import os
 
 import numpy as np
 import pytest
@@ -111,3 +112,25 @@ def test_decode_variants_match_twin(cuda, sg, oracle_paths, kw):
         assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i]),
                 int(stats["converged"][i]), int(stats["phases"][i])) == ts
         assert np.array_equal(lapp[i].view(np.int64), tl.view(np.int64))
+
+
+def test_random_mixed_codewords_match_twin(cuda, sg, oracle_paths):
+    """256 fresh codewords at per-codeword Eb/N0 ~ U[1, 3] dB, outside every
+    fixture: both the batched decoder (host entry point) and the plain
+    decoder (device entry point) equal the twin oracle in bits, every
+    statistic and every L_APP byte."""
+    torch = cuda
+    n = 256
+    _, llr = sg.gen_llr(4243, 0, n, ebn0_range=(1.0, 3.0))
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        ref = pool.map(twin_decode_one, [(oracle_paths["twin"], llr[i], {}) for i in range(n)])
+    hb, hs, hl = sg.decode(llr, want_lapp=True)
+    db, draw, dl = sg.decode(torch.from_numpy(llr).cuda(), want_lapp=True)
+    torch.cuda.synchronize()
+    ds, db, dl = sg.stats_from_device(draw), db.cpu().numpy(), dl.cpu().numpy()
+    for bits, stats, lapp in ((hb, hs, hl), (db, ds, dl)):
+        for i, (tb, ts, tl) in enumerate(ref):
+            assert np.array_equal(bits[i], tb), i
+            assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i]),
+                    int(stats["converged"][i]), int(stats["phases"][i])) == ts, i
+            assert np.array_equal(lapp[i].view(np.int64), tl.view(np.int64)), i
