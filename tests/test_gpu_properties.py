@@ -173,3 +173,25 @@ def test_guess_ceiling_bounds_the_decoder(cuda, sg):
     torch.cuda.synchronize()
     rate = sg.stats_from_device(raw)["ng"].sum() / (time.perf_counter() - t0)
     assert ceil.value > rate > 0
+
+
+def test_host_entry_point_from_two_threads(cuda, sg):
+    """sg_decode_host keeps its device buffers per device and serialises
+    calls on one device: two threads decoding different inputs at the same
+    time get exactly the results of one-at-a-time calls."""
+    import threading
+
+    ins = [sg.gen_llr(90 + k, 0, 40, ebn0_db=2.0)[1] for k in range(2)]
+    want = [sg.decode(x) for x in ins]
+    got = [None, None]
+
+    def run(k):
+        got[k] = sg.decode(ins[k])
+
+    threads = [threading.Thread(target=run, args=(k,)) for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for k in range(2):
+        assert np.array_equal(got[k][0], want[k][0]) and np.array_equal(got[k][1], want[k][1])
