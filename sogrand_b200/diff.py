@@ -9,7 +9,7 @@ APP against the transmitted code bits,
     loss = mean over codewords of sum_i softplus(s_i L_APP_i),  s_i = 2 c_i - 1,
 differentiated exactly on the branch of the forward pass (sorts, tested
 patterns, lists, stops, early terminations held fixed).  The plain decoder
-with the learned weights is then judged by BER.
+with the learned weights is then evaluated by BER.
 """
 from __future__ import annotations
 

@@ -1,4 +1,4 @@
-"""Learn per-phase extrinsic weights and judge them by BER against the plain
+"""Learn per-phase extrinsic weights and evaluate them by BER against the plain
 decoder.
 
     python -m sogrand_b200.learn --steps 60 --batch 4096 --train-ebn0 1.5 \
