@@ -103,59 +103,105 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def ref_inputs(td, n):
+    """LLR files for the CPU legs: codewords [0, n) of the bench stream, one
+    file per codeword.  They are made by the twin oracle's build of the
+    library's generator (bit-identical to sogrand_b200.gen_llr), so the
+    process timing the reference never loads the library."""
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "libsg_oracle_twin.so"))
+    lib.sgo_gen_llr.argtypes = [C.c_uint64, C.c_uint64, C.c_size_t, C.c_double, C.c_void_p, C.c_void_p]
+    lib.sgo_sigma.restype = C.c_double
+    lib.sgo_sigma.argtypes = [C.c_double]
+    sigma = lib.sgo_sigma(EBN0)
+    files = []
+    llr = np.zeros(4096)
+    for c in range(n):
+        lib.sgo_gen_llr(SEED, c, 1, sigma, None, llr.ctypes.data)
+        f = os.path.join(td, f"cw{c}.bin")
+        llr.tofile(f)
+        files.append(f)
+    return files
+
+
+def ref_kind():
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final_O2")
+    return ("reference", ref_bin) if os.path.exists(ref_bin) else ("port", None)
+
+
+def run_queue(files, workers, kind, ref_bin):
+    """Decode every file with `workers` concurrent decoders, each taking the
+    next codeword from a shared queue as soon as it is free (no core waits
+    on a fixed shard while others idle).  Returns the wall time."""
+    nxt = iter(files)
+    lock = threading.Lock()
+    failed = []
+
+    def worker():
+        while True:
+            with lock:
+                f = next(nxt, None)
+            if f is None:
+                return
+            if kind == "reference":
+                rc = subprocess.run([ref_bin, f, f + ".dec"], stdout=subprocess.DEVNULL).returncode
+            else:
+                rc = subprocess.run([sys.executable, __file__, "--port-worker", f]).returncode
+            if rc != 0:
+                failed.append(f)
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=worker) for _ in range(workers)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    dt = time.perf_counter() - t0
+    if failed:
+        raise RuntimeError(f"CPU decoder failed on {failed[:3]}")
+    return dt
+
+
+def cpu_sample_text(kind, n, per_core, cores):
+    who = ("an unmodified cubic_decoder_final process (reference source built at -O2)" if kind == "reference"
+           else "the oracle restatement")
+    return (f"{n} codewords per step ({per_core} per core) at {EBN0} dB; {cores} workers take one codeword "
+            f"at a time from a shared queue, each decoded by {who}")
+
+
 def run_reference(args, rank, world):
-    """CPU reference arm: rank 0 times the reference decoder on all host cores."""
+    """CPU reference arm: rank 0 times the reference decoder on all host
+    cores; the other ranks exit without work."""
     if rank != 0:
         return
-    import sogrand_b200 as sg
-
     cores = len(os.sched_getaffinity(0))
-    per_proc = args.ref_cw_per_core
-    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final_O2")
-    kind = "reference" if os.path.exists(ref_bin) else "port"
+    per_core = args.ref_cw_per_core
+    kind, ref_bin = ref_kind()
+    n = cores * per_core
     with tempfile.TemporaryDirectory() as td:
-        shards = []
-        for c in range(cores):
-            _, llr = sg.gen_llr(SEED, c * per_proc, per_proc, ebn0_db=EBN0)
-            f = os.path.join(td, f"llr{c}.bin")
-            llr.tofile(f)
-            shards.append(f)
-        times = []
-        for step in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            if kind == "reference":
-                procs = [subprocess.Popen([ref_bin, f, f + ".dec"], stdout=subprocess.DEVNULL) for f in shards]
-                for p in procs:
-                    if p.wait() != 0:
-                        raise RuntimeError("reference decoder failed")
-            else:
-                procs = [subprocess.Popen([sys.executable, __file__, "--port-worker", f]) for f in shards]
-                for p in procs:
-                    if p.wait() != 0:
-                        raise RuntimeError("oracle worker failed")
-            dt = time.perf_counter() - t0
-            if step >= args.warmup:
-                times.append(dt)
-    n = cores * per_proc
+        files = ref_inputs(td, n)
+        # warm-up steps (page in the binary and the inputs) decode one
+        # codeword per worker; the timed steps decode the whole sample
+        for _ in range(args.warmup):
+            run_queue(files[:cores], cores, kind, ref_bin)
+        times = [run_queue(files, cores, kind, ref_bin) for _ in range(args.steps)]
     value = n / statistics.mean(times)
-    sample = (f"{n} codewords per step ({per_proc} per core) at {EBN0} dB, one unmodified "
-              f"cubic_decoder_final process per core" if kind == "reference" else
-              f"{n} codewords per step ({per_proc} per core), oracle restatement per core")
+    sample = cpu_sample_text(kind, n, per_core, cores)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cubic (16,8)^3 SOGRAND decode, Eb/N0 {EBN0} dB, L=3 Imax=30 Tmax=inf",
-                   "sample": sample, "cores": cores},
+        "config": bench_config(args, args.n_cw, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "info_mbps": value * 512 / 1e6,
+        "step_seconds": {"min": min(times), "max": max(times)},
     }
     print(json.dumps(line), flush=True)
 
 
 def port_worker(path):
-    """Decode one LLR shard with the oracle restatement (CPU baseline leg)."""
+    """Decode one LLR file with the oracle restatement (CPU legs, used only
+    when the reference could not be built)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_api import Oracle
 
@@ -164,30 +210,26 @@ def port_worker(path):
 
 
 def cpu_baseline(args):
-    """Bounded CPU sample on the host cores: same kind as the reference arm."""
-    import sogrand_b200 as sg
-
+    """Bounded CPU sample on the host cores, the same measurement as the
+    reference arm's step."""
     cores = len(os.sched_getaffinity(0))
-    per_proc = args.cpu_cw_per_core
-    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final_O2")
-    kind = "reference" if os.path.exists(ref_bin) else "port"
+    per_core = args.cpu_cw_per_core
+    kind, ref_bin = ref_kind()
+    n = cores * per_core
     with tempfile.TemporaryDirectory() as td:
-        files = []
-        for c in range(cores):
-            _, llr = sg.gen_llr(SEED, c * per_proc, per_proc, ebn0_db=EBN0)
-            f = os.path.join(td, f"llr{c}.bin")
-            llr.tofile(f)
-            files.append(f)
-        t0 = time.perf_counter()
-        if kind == "reference":
-            procs = [subprocess.Popen([ref_bin, f, f + ".dec"], stdout=subprocess.DEVNULL) for f in files]
-        else:
-            procs = [subprocess.Popen([sys.executable, __file__, "--port-worker", f]) for f in files]
-        ok = all(p.wait() == 0 for p in procs)
-        dt = time.perf_counter() - t0
-    n = cores * per_proc
-    return {"value": n / dt if ok else None, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{n} codewords at {EBN0} dB ({per_proc} per core, one process per core), {dt:.1f} s wall"}
+        files = ref_inputs(td, n)
+        dt = run_queue(files, cores, kind, ref_bin)
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": cpu_sample_text(kind, n, per_core, cores) + f"; {dt:.1f} s wall"}
+
+
+def bench_config(args, n, world):
+    return {"workload": f"cubic (16,8)^3 SOGRAND decode, {n} codewords per GPU per step, "
+                        + (f"Eb/N0 {EBN0} dB" if args.workload == "2dB" else "Eb/N0 U[1,3] dB per codeword")
+                        + ", L=3 Imax=30 Tmax=inf",
+            "codewords_per_gpu": n, "ebn0_db": EBN0 if args.workload == "2dB" else [1.0, 3.0],
+            "form": args.form, "parallelism": f"replicas{world}",
+            "l2": f"inputs ({n * 32768 / 1e9:.1f} GB per GPU) larger than L2; no flush"}
 
 
 def main():
@@ -199,8 +241,8 @@ def main():
     ap.add_argument("--n-cw", type=int, default=100000, help="codewords per GPU per step")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-cw-per-core", type=int, default=16)
-    ap.add_argument("--ref-cw-per-core", type=int, default=4)
+    ap.add_argument("--cpu-cw-per-core", type=int, default=32)
+    ap.add_argument("--ref-cw-per-core", type=int, default=32)
     ap.add_argument("--form", default="batch", choices=["plain", "batch"],
                     help="plain: one CTA per codeword (sg_decode_device); batch: persistent kernel replayed "
                          "from a CUDA graph (sg_batch_*)")
@@ -335,12 +377,7 @@ def main():
             "vs_baseline_basis": f"{PUBLISHED_CW_PER_S} codewords/s, the reference's published GPU decoder "
                                  "figure at 2 dB (RTX 4070 Laptop, reference README.md:137-143)",
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"cubic (16,8)^3 SOGRAND decode, {n} codewords per GPU per step, "
-                                   + (f"Eb/N0 {EBN0} dB" if args.workload == "2dB" else "Eb/N0 U[1,3] dB per codeword")
-                                   + ", L=3 Imax=30 Tmax=inf",
-                       "codewords_per_gpu": n, "ebn0_db": EBN0 if args.workload == "2dB" else [1.0, 3.0],
-                       "form": args.form, "parallelism": f"replicas{world}",
-                       "l2": f"inputs ({n * 32768 / 1e9:.1f} GB per GPU) larger than L2; no flush"},
+            "config": bench_config(args, n, world),
             "info_mbps": value * 512 / 1e6,
             "ber": ber, "ng_per_codeword": ng_per_cw, "guesses_per_s": value * ng_per_cw,
             "guess_ceiling": {"bound": "fp64 exp per guess", "achieved": value * ng_per_cw / world,

@@ -78,7 +78,9 @@ typedef struct {
     uint64_t ng;       /* guesses, summed over all line decodes (NG) */
     uint64_t ng_p;     /* sum over phases of the largest line NG (NG_p) */
     int32_t converged; /* 1: early termination fired; 0: Imax reached;
-                          -1: input not finite, codeword not decoded */
+                          -1: input not finite, codeword not decoded;
+                          -2: not decoded because a bounded device wait
+                          gave up (see sg_check_device) */
     int32_t phases;    /* phases run */
 } sg_cw_stats;
 
@@ -96,9 +98,12 @@ typedef struct {
 void sg_params_default(sg_params* p);
 
 /* Decode n_cw LLR cubes on the GPU (device pointers, asynchronous).
- * d_llr must be 8-byte aligned (16-byte aligned uses bulk async copies).
+ * d_llr must be 8-byte aligned (16-byte aligned uses bulk async copies in
+ * the variants that stage the channel cube in shared memory).
  * d_lapp (nullable): final L_APP cubes, 4096 float64 per codeword.
- * d_stats (nullable): one sg_cw_stats per codeword.
+ * d_stats (nullable): one sg_cw_stats per codeword.  A codeword whose
+ * bulk-copy wait gave up is reported with converged = -2 and zero bits, and
+ * the device's error flag is set (sg_check_device).
  * Replaces the per-codeword loop of main(), cubic_decoder_final.c:119-289. */
 sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
                            uint8_t* d_bits, double* d_lapp, sg_cw_stats* d_stats,
@@ -149,6 +154,15 @@ typedef struct {
     uint64_t bit_errors;      /* decoded info bits differing from ref_info */
     uint64_t block_errors;    /* codewords with at least one bit error */
     double total_iterations;  /* sum of per-codeword iterations (exact) */
+    uint64_t timeouts;        /* codewords not decoded because a bounded
+                                 device wait gave up (converged = -2) */
+    uint32_t device_error;    /* the library's device error flags when the
+                                 summary was formed: bit 0 a bulk-copy wait
+                                 gave up, bit 1 that copy never completed.
+                                 The allocation-free entry point reports its
+                                 own call's flags; the regular one reports the
+                                 device's flags since the last sg_check_device */
+    uint32_t reserved;
 } sg_decode_summary;
 
 /* Decode and reduce on the device: bits (nullable: not returned) and one
@@ -271,6 +285,26 @@ int sg_decoder_variant_count(void);
 const char* sg_decoder_variant_name(int v);
 sg_status sg_decoder_set_variant(int v);
 int sg_decoder_get_variant(void);
+
+/* ---- device-side waits.  Every wait in the library's kernels is bounded.
+ * A bulk-copy wait that gives up marks its CTA's remaining codewords
+ * converged = -2 and sets the device's error flag; a persistent-decoder warp
+ * that finds no work for too long exits and sets its batch's flag
+ * (sg_batch_check; the other warps finish the batch).  The limit applies to
+ * launches made after the call, process-wide: polls of a bulk-copy wait,
+ * idle rounds of a persistent warp.  The default, and the largest value
+ * accepted (larger values are clamped), is 2^22.  A limit of 0 makes every
+ * wait that is not already complete give up; it exists so that tests can
+ * exercise the error paths without a faulty GPU. */
+sg_status sg_set_wait_limit(uint64_t limit);
+uint64_t sg_get_wait_limit(void);
+
+/* Synchronise `stream`, then read and clear the current device's error
+ * flag: SG_ERR_TIMEOUT if a bounded wait of a plain-decoder kernel
+ * (sg_decode_device, sg_decode_summary_device, sg_forward_device) gave up
+ * since the last check, SG_OK otherwise.  The flag is shared by all
+ * streams of the device. */
+sg_status sg_check_device(void* stream);
 
 /* ---- diagnostics */
 

@@ -26,6 +26,9 @@ int early_termination(ref_tensor_d L_APP, int** G, int n, int k);
 void hard_decision(double* llr, int* bits, int length);
 void SOGRAND_bitSO(double* L_APP, double* L_E, int* N_guess, double* llr, int** H_matrix,
                    int n, int k, int L, uint64_t Tmax, double thres, int even);
+void sogrand_main_logic(double* chat_list, double* s_list, double* T_val, double* curL_val, double* pNL_val,
+                        double* APP_list, double* llr, uint8_t* H_flat, int n, int s, int IC, uint64_t L,
+                        uint64_t Tmax, double thres, int even);
 
 static int** g_G;
 static int** g_H;
@@ -74,6 +77,28 @@ void sgref_bitso(const double* llr, int L, uint64_t Tmax, double thres,
     SOGRAND_bitSO(lapp, le, n_guess, v, g_H, 16, 8, L, Tmax, thres, g_even);
 }
 
+/* Whether SOGRAND_bitSO on this line reads its uninitialised list size
+ * (cubic_decoder_final.c:524, :536): the reference's sogrand_main_logic is
+ * run with that output preset to -1, and a line whose search lists no
+ * codeword (possible only under a finite Tmax) leaves it there.  Returns 1
+ * for such a line, 0 otherwise; *T_out (nullable) receives its T. */
+int sgref_line_undefined(const double* llr, int L, uint64_t Tmax, double thres, double* T_out)
+{
+    init();
+    double v[16], chat[16 * 8], sl[4 * 8], app[8], T = 0, curl = -1.0, pnl = 0;
+    uint8_t hf[8 * 16];
+    if (L < 1 || L > 8)
+        return -1;
+    memcpy(v, llr, sizeof v);
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 16; j++)
+            hf[i * 16 + j] = (uint8_t)g_H[i][j];
+    sogrand_main_logic(chat, sl, &T, &curl, &pnl, app, v, hf, 16, 8, -1, (uint64_t)L, Tmax, thres, g_even);
+    if (T_out)
+        *T_out = T;
+    return curl == -1.0;
+}
+
 int sgref_early_termination(const double* lapp)
 {
     init();
@@ -84,9 +109,31 @@ int sgref_early_termination(const double* lapp)
 /* Decode n_cw cubes with the reference's functions.  alpha has 100 entries
  * indexed as the reference does (alpha[2*iter-2] columns, alpha[2*iter-1]
  * rows and slices).  Any output pointer may be NULL. */
+static void decode_impl(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax, double thres,
+                        const double* alpha, uint8_t* bits, double* lapp_out, double* iters, uint64_t* ng_out,
+                        uint64_t* ngp_out, int* conv_out, int* undef_out);
+
 void sgref_decode(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax,
                   double thres, const double* alpha, uint8_t* bits, double* lapp_out,
                   double* iters, uint64_t* ng_out, uint64_t* ngp_out, int* conv_out)
+{
+    decode_impl(llr, n_cw, L, Imax, Tmax, thres, alpha, bits, lapp_out, iters, ng_out, ngp_out, conv_out, NULL);
+}
+
+/* sgref_decode that also counts, per codeword, the line decodes that read
+ * the reference's uninitialised list size (sgref_line_undefined); the
+ * codeword's outputs are undefined when the count is not 0. */
+void sgref_decode_checked(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax,
+                          double thres, const double* alpha, uint8_t* bits, double* lapp_out,
+                          double* iters, uint64_t* ng_out, uint64_t* ngp_out, int* conv_out, int* undef_out)
+{
+    decode_impl(llr, n_cw, L, Imax, Tmax, thres, alpha, bits, lapp_out, iters, ng_out, ngp_out, conv_out,
+                undef_out);
+}
+
+static void decode_impl(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax, double thres,
+                        const double* alpha, uint8_t* bits, double* lapp_out, double* iters, uint64_t* ng_out,
+                        uint64_t* ngp_out, int* conv_out, int* undef_out)
 {
     init();
     const int n = 16, N3 = 4096;
@@ -102,7 +149,7 @@ void sgref_decode(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax
         memset(lapp, 0, sizeof(double) * N3);
         memset(le, 0, sizeof(double) * N3);
         double n_iter = 0;
-        int NG = 0, NG_p = 0, conv = 0;
+        int NG = 0, NG_p = 0, conv = 0, undef = 0;
         for (int iter = 1; iter <= Imax && !conv; iter++) {
             for (int ph = 0; ph < 3 && !conv; ph++) {
                 int NGmax = 0;
@@ -121,6 +168,8 @@ void sgref_decode(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax
                         for (int i = 0; i < n; i++)
                             vin[i] = in[base + i * st];
                         int ngs = 0;
+                        if (undef_out)
+                            undef += sgref_line_undefined(vin, L, Tmax, thres, NULL) == 1;
                         SOGRAND_bitSO(vapp, vle, &ngs, vin, g_H, n, 8, L, Tmax, thres, g_even);
                         NG += ngs;
                         if (ngs > NGmax)
@@ -140,6 +189,7 @@ void sgref_decode(const double* llr, size_t n_cw, int L, int Imax, uint64_t Tmax
         if (ng_out) ng_out[cw] = (uint64_t)(unsigned)NG;
         if (ngp_out) ngp_out[cw] = (uint64_t)(unsigned)NG_p;
         if (conv_out) conv_out[cw] = conv;
+        if (undef_out) undef_out[cw] = undef;
         if (bits) {
             hard_decision(lapp, hb, 512);
             uint8_t* o = bits + cw * 64;

@@ -21,7 +21,46 @@
 #define SGO_TWIN 0
 #endif
 
-#if SGO_TWIN
+#ifndef SGO_CRQ
+#define SGO_CRQ 0
+#endif
+
+#if SGO_CRQ
+/* Correctly rounded exp/log, as a checker: x87 extended precision first
+ * (about 2^-62 relative error), and, when that result lies within 2^-60 of
+ * the midpoint between two doubles, binary128 (libquadmath) rounded once to
+ * double.  Slow and host-only; it serves to measure what a correctly
+ * rounded libm changes and to check correctly rounded implementations. */
+#include <quadmath.h>
+static double crq_round(long double y, double x, int is_exp)
+{
+    double d = (double)y; /* round to nearest */
+    if (!(d == d) || d == 0.0 || d > 1.7976931348623157e308 || d < -1.7976931348623157e308)
+        return d;
+    long double diff = y - (long double)d;
+    double nb = nextafter(d, diff > 0 ? INFINITY : -INFINITY);
+    long double half = fabsl((long double)nb - (long double)d) / 2;
+    if (fabsl(fabsl(diff) - half) > ldexpl(fabsl(y), -60))
+        return d;
+    __float128 q = is_exp ? expq((__float128)x) : logq((__float128)x);
+    return (double)q;
+}
+static double ox_exp(double x)
+{
+    if (!(x <= 709.782712893384))
+        return x != x ? x : INFINITY;
+    if (x < -745.2)
+        return 0.0;
+    return crq_round(expl((long double)x), x, 1);
+}
+static double ox_log(double x)
+{
+    if (!(x > 0.0) || x > 1.7976931348623157e308)
+        return log(x);
+    return crq_round(logl((long double)x), x, 0);
+}
+static double ox_pow2_neg(double s) { return pow(2.0, -s); }
+#elif SGO_TWIN
 #include "../sogrand_b200/csrc/sg_math.h"
 static const double k_etab[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
 static const double k_ltab[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
@@ -42,7 +81,7 @@ static double ox_log(double x) { return log(x); }
 static double ox_pow2_neg(double s) { return pow(2.0, -s); }
 #endif
 
-int sgo_math_mode(void) { return SGO_TWIN; }
+int sgo_math_mode(void) { return SGO_CRQ ? 2 : SGO_TWIN; }
 
 static const double kEps = 1e-40; /* EPSILON, D:16 */
 
@@ -179,6 +218,7 @@ typedef struct {
     uint8_t cHD[SGO_N];
     int perm[SGO_N];
     double absL[SGO_N]; /* sorted ascending after the sort */
+    double delta[SGO_N]; /* JacLog(|L|) - JacLog(-|L|) per sorted position */
     double pm_hd;
     double p_not_guess;
     double T;           /* T_val, a double in the reference */
@@ -193,13 +233,16 @@ typedef struct {
     double epos[SGO_N];   /* the same over guesses that flip position i */
 } line_state;
 
-/* PM of a test error pattern over sorted positions (getPM, D:765). */
+/* PM of a test error pattern over sorted positions (getPM, D:765).  The
+ * reference evaluates the parenthesised difference of JacLogs afresh for
+ * every pattern; it is a pure function of the position, so the per-line
+ * value in delta[] is the same number. */
 static double pattern_pm(const line_state* s, const uint8_t tep[SGO_N])
 {
     double pm = s->pm_hd;
     for (int i = 0; i < SGO_N; i++)
         if (tep[i] == 1)
-            pm += (jaclog(s->absL[i]) - jaclog(-s->absL[i]));
+            pm += s->delta[i];
     return pm;
 }
 
@@ -352,6 +395,8 @@ static void main_logic(line_state* s, const double llr[SGO_N])
         pm += jaclog(-s->absL[i]);
     s->pm_hd = pm;
     qsort_ref(s->absL, s->perm, n);
+    for (int i = 0; i < n; i++)
+        s->delta[i] = (jaclog(s->absL[i]) - jaclog(-s->absL[i]));
     double beta = (s->absL[(uint64_t)round((double)n / 2) - 1] - s->absL[0]) / (round((double)n / 2) - 1);
     int32_t ic = cvt_i32(round(s->absL[0] / beta - 1));
     if (ic < 0)
@@ -805,6 +850,35 @@ double sgo_decode_loss(const double* llr, const sgo_params* p, const uint8_t* co
     free(lapp);
     return loss;
 }
+
+#if SGO_TWIN
+#include "../sogrand_b200/csrc/sg_gen.h"
+/* The seeded channel output of the library's generator (sg_gen.h, compiled
+ * here from the same source with the same exp/log) for codewords
+ * [cw0, cw0+n) at noise deviation sigma: packed info bytes (nullable) and
+ * LLR cubes.  Encoding uses this file's restatement of cubic_encoder.c.
+ * Lets the CPU timing legs prepare the reference's inputs without loading
+ * the library. */
+void sgo_gen_llr(uint64_t seed, uint64_t cw0, size_t n, double sigma, uint8_t* info, double* llr)
+{
+    uint8_t ib[SGO_INFO / 8], bits[SGO_INFO], cw[SGO_CUBE];
+    for (size_t c = 0; c < n; c++) {
+        const uint64_t gc = cw0 + c;
+        for (int w = 0; w < 8; w++) {
+            const uint64_t r = sg_rand(seed, 0, gc * 8 + (uint64_t)w);
+            for (int q = 0; q < 8; q++)
+                ib[w * 8 + q] = (uint8_t)(r >> (8 * q));
+        }
+        if (info)
+            memcpy(info + c * (SGO_INFO / 8), ib, SGO_INFO / 8);
+        for (int b = 0; b < SGO_INFO; b++) /* packed MSB first, as generate_bin/comparator files */
+            bits[b] = (uint8_t)((ib[b >> 3] >> (7 - (b & 7))) & 1);
+        sgo_encode(bits, cw);
+        for (int p = 0; p < SGO_CUBE; p++)
+            llr[c * SGO_CUBE + p] = sg_llr_of(cw[p], sigma, sg_normal(seed, gc, (uint32_t)p, k_ltab));
+    }
+}
+#endif
 
 double sgo_sigma(double ebn0_db) /* C:34-39, code_dim = 3 */
 {

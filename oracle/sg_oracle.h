@@ -81,6 +81,10 @@ void sgo_encode(const uint8_t info[SGO_INFO], uint8_t cw[SGO_CUBE]);
 /* Noise standard deviation of channel_sim.c:34-39 for code dimension 3. */
 double sgo_sigma(double ebn0_db);
 
+/* Twin build only (libsg_oracle_twin.so): the library generator's seeded
+ * channel output, for preparing reference inputs without the library. */
+void sgo_gen_llr(uint64_t seed, uint64_t cw0, size_t n, double sigma, uint8_t* info, double* llr);
+
 /* FP64 adjoint of one codeword's decode (the branch of the forward pass
  * held fixed): loss = sum_i softplus(s_i L_APP_i) over the 4096 code bits,
  * s_i = +1 for bit 1, -1 for 0; grad_alpha[3*Imax] and grad_llr[4096] its

@@ -24,7 +24,7 @@ from ._lib import (SG_CUBE, SG_INFO_BYTES, SG_MAX_PHASES, SgCwStats, SgParams,
 __all__ = [
     "SG_CUBE", "SG_INFO_BYTES", "STATS_DTYPE", "SograndError", "params", "reference_alpha",
     "decode", "bitso", "decode_file", "decode_summary", "wilson_interval", "SUMMARY_DTYPE", "channel_sigma", "gen_info", "encode", "gen_llr",
-    "version",
+    "set_wait_limit", "get_wait_limit", "check_device", "version",
 ]
 
 UINT64_MAX = (1 << 64) - 1
@@ -138,7 +138,8 @@ def decode_file(in_path: str, out_path: str, p: SgParams | None = None, chunk_cw
 
 SUMMARY_DTYPE = np.dtype([("blocks", "<u8"), ("converged", "<u8"), ("nonfinite", "<u8"), ("total_ng", "<u8"),
                           ("total_ng_p", "<u8"), ("bits_compared", "<u8"), ("bit_errors", "<u8"),
-                          ("block_errors", "<u8"), ("total_iterations", "<f8")])
+                          ("block_errors", "<u8"), ("total_iterations", "<f8"), ("timeouts", "<u8"),
+                          ("device_error", "<u4"), ("reserved", "<u4")])
 
 
 def decode_summary(llr, p: SgParams | None = None, ref_info=None, want_bits: bool = False, stream=None):
@@ -156,6 +157,23 @@ def decode_summary(llr, p: SgParams | None = None, ref_info=None, want_bits: boo
     check(_lib.load().sg_decode_summary_device(_ptr(llr), n, C.byref(p), _ptr(ref_info), _ptr(bits), _ptr(summ), s))
     rec = np.frombuffer(summ.cpu().numpy().tobytes(), dtype=SUMMARY_DTYPE)[0]
     return {k: rec[k].item() for k in SUMMARY_DTYPE.names}, bits
+
+
+def set_wait_limit(limit: int) -> None:
+    """Polls / idle rounds before a device-side wait gives up, for launches
+    made after the call (process-wide; default and maximum 2^22)."""
+    check(_lib.load().sg_set_wait_limit(int(limit)))
+
+
+def get_wait_limit() -> int:
+    return int(_lib.load().sg_get_wait_limit())
+
+
+def check_device(stream=None) -> None:
+    """Synchronise `stream` and raise SograndError(SG_ERR_TIMEOUT) if a
+    bounded wait of a plain-decoder kernel gave up on the current device
+    since the last check (the flag is cleared)."""
+    check(_lib.load().sg_check_device(stream))
 
 
 def wilson_interval(k: int, n: int, conf_z: float = 1.959963984540054) -> tuple[float, float]:

@@ -73,6 +73,9 @@ class SgDecodeSummary(C.Structure):
         ("bit_errors", C.c_uint64),
         ("block_errors", C.c_uint64),
         ("total_iterations", C.c_double),
+        ("timeouts", C.c_uint64),
+        ("device_error", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -98,6 +101,9 @@ _SIGS = {
         [C.c_uint64, C.c_uint64, C.c_size_t, C.c_double, C.c_double, C.c_double, _VP, _VP, _VP],
     ),
     "sg_pattern_order": (C.c_size_t, [C.c_int32, _VP, C.c_size_t]),
+    "sg_set_wait_limit": (C.c_int, [C.c_uint64]),
+    "sg_get_wait_limit": (C.c_uint64, []),
+    "sg_check_device": (C.c_int, [_VP]),
     "sg_guess_ceiling": (C.c_int, [C.c_ulonglong, C.POINTER(C.c_double)]),
     "sg_forward_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP, _VP]),
     "sg_backward_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),

@@ -25,6 +25,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <chrono>
 #include <mutex>
 #include <new>
@@ -40,7 +41,14 @@
 
 #define SG_THREADS 256
 #define SG_WARPS (SG_THREADS / 32)
-#define SG_SPIN_LIMIT (1ll << 22) /* bounded mbarrier polling */
+/* Bounded device-side waits.  The limit of a wait that can give up (the
+ * bulk-copy wait here, the persistent decoder's idle rounds) is a launch
+ * argument, SG_WAIT_LIMIT_DEFAULT unless sg_set_wait_limit() changed it.
+ * After a bulk-copy wait gave up, the copy may still be writing into the
+ * CTA's shared memory: the CTA waits for it again, up to SG_DRAIN_LIMIT
+ * polls, before it releases that memory. */
+#define SG_WAIT_LIMIT_DEFAULT (1ll << 22)
+#define SG_DRAIN_LIMIT (1ll << 26)
 
 __device__ const double g_etab[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
 __device__ const double g_ltab[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
@@ -56,6 +64,7 @@ struct SgDecodeArgs {
     unsigned int* err;
     double* ckpt; /* nullable: [n_cw][3*imax][4096], L_E entering each phase */
     unsigned long long n_cw;
+    long long wait_limit; /* polls or idle rounds before a bounded wait gives up */
     int32_t L;
     int32_t imax;
     uint32_t tmax;
@@ -63,6 +72,39 @@ struct SgDecodeArgs {
     double thres;
     double alpha[SG_MAX_PHASES];
 };
+
+/* Poll the mbarrier for phase `parity` at most `limit` times; 1 when it
+ * completed. */
+__device__ __forceinline__ uint32_t sg_mbar_wait(uint32_t mbar, uint32_t parity, long long limit)
+{
+    uint32_t ok = 0;
+    for (long long it = 0; it < limit && !ok; it++) {
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(ok)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+    }
+    return ok;
+}
+
+/* Outputs of a codeword that is not decoded: zero bits and statistics with
+ * the given converged code (-1 non-finite input, -2 a wait gave up).
+ * Called by the whole CTA. */
+__device__ __forceinline__ void sg_cw_not_decoded(const SgDecodeArgs& args, unsigned long long cw, int code)
+{
+    if (threadIdx.x < SG_INFO_BYTES)
+        args.bits[cw * SG_INFO_BYTES + threadIdx.x] = 0;
+    if (threadIdx.x == 0 && args.stats) {
+        sg_cw_stats st;
+        st.iterations = 0;
+        st.ng = 0;
+        st.ng_p = 0;
+        st.converged = code;
+        st.phases = 0;
+        args.stats[cw] = st;
+    }
+}
 
 /* Shared memory of a decode CTA.  With LCH_SMEM the channel cube is staged
  * here by one bulk copy; otherwise each line reads its 16 channel LLRs from
@@ -185,38 +227,29 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
             S.bad = 0;
         }
         if (use_bulk && tid == 0) {
-            uint32_t ok = 0;
-            for (long long it = 0; it < SG_SPIN_LIMIT && !ok; it++) {
-                asm volatile(
-                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                    : "=r"(ok)
-                    : "r"(mbar), "r"(phase_bit)
-                    : "memory");
-            }
-            if (!ok) {
+            if (!sg_mbar_wait(mbar, phase_bit, args.wait_limit)) {
+                /* gave up: report it, then let the copy land before this
+                 * CTA's shared memory is reused or released */
                 atomicOr(args.err, 1u);
+                if (!sg_mbar_wait(mbar, phase_bit, SG_DRAIN_LIMIT))
+                    atomicOr(args.err, 2u);
                 S.bad = 2;
             }
         }
         phase_bit ^= 1u;
         __syncthreads();
-        if (S.bad == 2) /* the bulk copy never completed: skip this codeword */
-            break;
+        if (S.bad == 2) {
+            /* this codeword and the CTA's later ones are reported as not
+             * decoded (converged = -2) */
+            for (unsigned long long c = cw; c < args.n_cw; c += gridDim.x)
+                sg_cw_not_decoded(args, c, -2);
+            return;
+        }
         bool nonfinite = false;
         for (int i = tid; i < SG_CUBE; i += NT)
             nonfinite |= !isfinite(LCH_SMEM ? S.lch[i] : __ldg(g + i));
         if (__syncthreads_or(nonfinite)) {
-            if (tid < SG_INFO_BYTES)
-                args.bits[cw * SG_INFO_BYTES + tid] = 0;
-            if (tid == 0 && args.stats) {
-                sg_cw_stats st;
-                st.iterations = 0;
-                st.ng = 0;
-                st.ng_p = 0;
-                st.converged = -1;
-                st.phases = 0;
-                args.stats[cw] = st;
-            }
+            sg_cw_not_decoded(args, cw, -1);
             __syncthreads();
             continue;
         }
@@ -408,15 +441,17 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
 __global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __restrict__ stats,
                                                           const uint8_t* __restrict__ bits,
                                                           const uint8_t* __restrict__ ref,
-                                                          unsigned long long n, sg_decode_summary* out)
+                                                          unsigned long long n, const unsigned int* err,
+                                                          sg_decode_summary* out)
 {
-    unsigned long long conv = 0, nonf = 0, ng = 0, ngp = 0, be = 0, ble = 0;
+    unsigned long long conv = 0, nonf = 0, tmo = 0, ng = 0, ngp = 0, be = 0, ble = 0;
     double it = 0.0;
     for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
          c += (unsigned long long)gridDim.x * blockDim.x) {
         const sg_cw_stats st = stats[c];
         conv += st.converged == 1;
-        nonf += st.converged < 0;
+        nonf += st.converged == -1;
+        tmo += st.converged == -2;
         ng += st.ng;
         ngp += st.ng_p;
         it += st.iterations;
@@ -435,6 +470,7 @@ __global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __re
     for (int off = 16; off > 0; off >>= 1) {
         conv += __shfl_xor_sync(SG_FULL, conv, off);
         nonf += __shfl_xor_sync(SG_FULL, nonf, off);
+        tmo += __shfl_xor_sync(SG_FULL, tmo, off);
         ng += __shfl_xor_sync(SG_FULL, ng, off);
         ngp += __shfl_xor_sync(SG_FULL, ngp, off);
         be += __shfl_xor_sync(SG_FULL, be, off);
@@ -444,6 +480,7 @@ __global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __re
     if ((threadIdx.x & 31) == 0) {
         atomicAdd((unsigned long long*)&out->converged, conv);
         atomicAdd((unsigned long long*)&out->nonfinite, nonf);
+        atomicAdd((unsigned long long*)&out->timeouts, tmo);
         atomicAdd((unsigned long long*)&out->total_ng, ng);
         atomicAdd((unsigned long long*)&out->total_ng_p, ngp);
         atomicAdd((unsigned long long*)&out->bit_errors, be);
@@ -452,6 +489,8 @@ __global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __re
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd((unsigned long long*)&out->blocks, n);
+        if (err)
+            out->device_error = *(volatile const unsigned int*)err;
         if (ref)
             atomicAdd((unsigned long long*)&out->bits_compared, n * (unsigned long long)SG_INFO_BITS);
     }
@@ -605,6 +644,7 @@ struct DevCtx {
 };
 
 std::mutex g_mu;
+std::atomic<long long> g_wait_limit{SG_WAIT_LIMIT_DEFAULT};
 int g_pvariant = 5; /* p32x3-g2: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
 int g_variant = 4; /* w16-gmem-g2: fastest on B200 at 2 dB (sogrand_b200.autotune) */
 DevCtx g_ctx[64];
@@ -738,6 +778,7 @@ sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
     a.enum_tabs = c->enum_tabs;
     a.err = c->err;
     a.n_cw = n_cw;
+    a.wait_limit = g_wait_limit.load();
     a.L = p->L;
     a.imax = p->Imax;
     a.tmax = tmax_eff(p->Tmax);
@@ -999,11 +1040,14 @@ sg_status sg_decode_summary_device(const double* d_llr, size_t n_cw, const sg_pa
     uint8_t* bits = d_bits ? d_bits : scratch + stat_bytes;
     s = sg_decode_device(d_llr, n_cw, p, bits, nullptr, stats, stream);
     if (s == SG_OK) {
-        sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw,
-                                                                                  d_summary);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess)
-            s = cuda_fail(e, "summary kernel");
+        DevCtx* c = nullptr;
+        if ((s = get_ctx(&c)) == SG_OK) {
+            sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info,
+                                                                                      n_cw, c->err, d_summary);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess)
+                s = cuda_fail(e, "summary kernel");
+        }
     }
     cudaError_t e = cudaFreeAsync(scratch, st);
     if (s == SG_OK && e != cudaSuccess)
@@ -1114,6 +1158,7 @@ sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, con
     a.enum_tabs = c->enum_tabs;
     a.err = err;
     a.n_cw = n_cw;
+    a.wait_limit = g_wait_limit.load();
     a.L = p->L;
     a.imax = p->Imax;
     a.tmax = tmax_eff(p->Tmax);
@@ -1123,7 +1168,7 @@ sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, con
     const SgVariant& v = g_variants[g_variant];
     void* kargs[] = {(void*)&a};
     SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid_for(n_cw, 1 << 30)), dim3(v.nw * 32), kargs, v.smem, st));
-    sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw,
+    sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw, err,
                                                                               d_summary);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
@@ -1170,6 +1215,7 @@ sg_status batch_enqueue(sg_batch b, const double* d_llr, size_t n_cw, const sg_p
     a.enum_tabs = c->enum_tabs;
     a.err = c->err;
     a.n_cw = n_cw;
+    a.wait_limit = g_wait_limit.load();
     a.L = p->L;
     a.imax = p->Imax;
     a.tmax = tmax_eff(p->Tmax);
@@ -1487,6 +1533,7 @@ sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p
     a.err = c->err;
     a.ckpt = d_ckpt;
     a.n_cw = n_cw;
+    a.wait_limit = g_wait_limit.load();
     a.L = p->L;
     a.imax = p->Imax;
     a.tmax = tmax_eff(p->Tmax);
@@ -1534,6 +1581,32 @@ sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* 
     void* kargs[] = {(void*)&a};
     SG_CUDA(cudaLaunchKernel((const void*)sg_backward_kernel<8>, dim3(grid_for(n_cw, 1 << 30)), dim3(256), kargs,
                              sizeof(SgBackSmem<8>), (cudaStream_t)stream));
+    return SG_OK;
+}
+
+sg_status sg_set_wait_limit(uint64_t limit)
+{
+    g_wait_limit.store(limit > (uint64_t)SG_WAIT_LIMIT_DEFAULT ? SG_WAIT_LIMIT_DEFAULT : (long long)limit);
+    return SG_OK;
+}
+
+uint64_t sg_get_wait_limit(void) { return (uint64_t)g_wait_limit.load(); }
+
+sg_status sg_check_device(void* stream)
+{
+    DevCtx* c = nullptr;
+    sg_status s = get_ctx(&c);
+    if (s != SG_OK)
+        return s;
+    SG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    unsigned int flags = 0;
+    SG_CUDA(cudaMemcpy(&flags, c->err, sizeof flags, cudaMemcpyDeviceToHost));
+    if (flags) {
+        SG_CUDA(cudaMemset(c->err, 0, sizeof flags));
+        return fail(SG_ERR_TIMEOUT, (flags & 2u) ? "a bulk-copy wait gave up and the copy did not complete"
+                                                 : "a bulk-copy wait gave up; the affected codewords report "
+                                                   "converged = -2");
+    }
     return SG_OK;
 }
 

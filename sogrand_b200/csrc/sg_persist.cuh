@@ -15,11 +15,11 @@
  * outputs are bit-identical to the plain decoder's.
  *
  * Waits are bounded: a warp that finds no line sleeps and retries; after
- * SG_IDLE_LIMIT consecutive idle rounds it records an error and exits.
+ * args.wait_limit consecutive idle rounds it records an error (SgQueue.err)
+ * and exits.  The warps that hold lines are never the ones that give up, so
+ * the batch still completes with the remaining warps.
  */
 #pragma once
-
-#define SG_IDLE_LIMIT (1 << 22)
 
 struct SgSlot {
     double le[SG_CUBE];
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(NW * 32, 1) sg_persist_kernel(const __grid_con
                 live |= sg_ld_volatile(&S.slot[c].cw) >= 0;
             if (!live)
                 break;
-            if (++idle > SG_IDLE_LIMIT) {
+            if (++idle > args.wait_limit) {
                 if (lane == 0)
                     atomicOr(&q->err, 2u);
                 break;

@@ -50,7 +50,12 @@ SETS = [
     ("snr_2.5dB", 103, 24, 2.5, UINT64_MAX),
     ("snr_3.0dB", 104, 24, 3.0, UINT64_MAX),
     ("mixed_1to3dB", 105, 24, (1.0, 3.0), UINT64_MAX),
+    # the Tmax-capped mode (the cap is checked once per logistic weight)
+    ("tmax1000_2dB", 106, 64, 2.0, 1000),
+    ("tmax1000_1.5dB", 107, 64, 1.5, 1000),
 ]
+# per-line known answers under a Tmax cap
+KAT_TMAX = (10, 100, 1000)
 
 
 def sha(b: bytes) -> str:
@@ -76,24 +81,27 @@ class Stats(C.Structure):
 
 
 def ref_one(args):
-    """Reference decode of one codeword -> (bits, iters, ng, ngp, conv, lapp sha)."""
+    """Reference decode of one codeword -> (bits, iters, ng, ngp, conv, lapp
+    sha, line decodes that read the reference's uninitialised list size)."""
     llr, tmax = args
     lib = C.CDLL(REF_SO)
     dp = np.ctypeslib.ndpointer(np.float64, flags="C")
     u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
     u64 = np.ctypeslib.ndpointer(np.uint64, flags="C")
     i32 = np.ctypeslib.ndpointer(np.int32, flags="C")
-    lib.sgref_decode.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp, u8, dp, dp,
-                                 u64, u64, i32]
+    lib.sgref_decode_checked.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp, u8, dp,
+                                         dp, u64, u64, i32, i32]
     bits = np.zeros(64, np.uint8)
     lapp = np.zeros(4096)
     it = np.zeros(1)
     ng = np.zeros(1, np.uint64)
     ngp = np.zeros(1, np.uint64)
     cv = np.zeros(1, np.int32)
-    lib.sgref_decode(np.ascontiguousarray(llr), 1, 3, 30, tmax, THRES, np.full(100, 0.7), bits, lapp, it, ng,
-                     ngp, cv)
-    return bits.tobytes().hex(), float(it[0]), int(ng[0]), int(ngp[0]), int(cv[0]), sha(lapp.tobytes())
+    und = np.zeros(1, np.int32)
+    lib.sgref_decode_checked(np.ascontiguousarray(llr), 1, 3, 30, tmax, THRES, np.full(100, 0.7), bits, lapp, it,
+                             ng, ngp, cv, und)
+    return (bits.tobytes().hex(), float(it[0]), int(ng[0]), int(ngp[0]), int(cv[0]), sha(lapp.tobytes()),
+            int(und[0]))
 
 
 def twin_one(args):
@@ -167,7 +175,8 @@ def main():
                 "llr_sha256": sha(llr.tobytes()), "info_sha256": sha(info.tobytes()),
                 "ref": {"bits": [r[0] for r in ref], "iterations": [r[1] for r in ref],
                         "ng": [r[2] for r in ref], "ng_p": [r[3] for r in ref],
-                        "converged": [r[4] for r in ref], "lapp_sha256": [r[5] for r in ref]},
+                        "converged": [r[4] for r in ref], "lapp_sha256": [r[5] for r in ref],
+                        "undefined_lines": [r[6] for r in ref]},
                 "twin": {"bits": [r[0] for r in twin], "iterations": [r[1] for r in twin],
                          "ng": [r[2] for r in twin], "ng_p": [r[3] for r in twin],
                          "converged": [r[4] for r in twin], "lapp_sha256": [r[5] for r in twin]},
@@ -205,18 +214,32 @@ def main():
     ref = C.CDLL(REF_SO)
     dp = np.ctypeslib.ndpointer(np.float64, flags="C")
     ref.sgref_bitso.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, dp, dp, C.POINTER(C.c_int)]
+    ref.sgref_line_undefined.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, C.POINTER(C.c_double)]
     kat = {"llr": lines}
-    for L, tmax, tag in ((3, UINT64_MAX, "L3"), (1, UINT64_MAX, "L1"), (4, UINT64_MAX, "L4")):
+    runs = [(3, UINT64_MAX, "L3"), (1, UINT64_MAX, "L1"), (4, UINT64_MAX, "L4")]
+    runs += [(3, t, f"T{t}") for t in KAT_TMAX]
+    for L, tmax, tag in runs:
         lapp = np.zeros_like(lines)
         le = np.zeros_like(lines)
         ng = np.zeros(len(lines), np.int32)
+        undef = np.zeros(len(lines), np.int8)
         for i in range(len(lines)):
             a = np.zeros(16)
             b = np.zeros(16)
             k = C.c_int()
+            # a line that lists no codeword makes the reference read its
+            # uninitialised list size: its soft output is undefined there
+            # (only N_guess is), and is recorded as NaN
+            undef[i] = ref.sgref_line_undefined(lines[i], L, tmax, THRES, None)
             ref.sgref_bitso(lines[i], L, tmax, THRES, a, b, C.byref(k))
+            if undef[i]:
+                a[:] = np.nan
+                b[:] = np.nan
             lapp[i], le[i], ng[i] = a, b, k.value
         kat[f"{tag}_lapp"], kat[f"{tag}_le"], kat[f"{tag}_nguess"] = lapp, le, ng
+        if tmax != UINT64_MAX:
+            kat[f"{tag}_undefined"] = undef
+            print(f"KAT Tmax={tmax}: {int(undef.sum())} of {len(lines)} lines list no codeword", flush=True)
     np.savez_compressed(os.path.join(OUT_DIR, "kat_lines.npz"), **kat)
     with open(os.path.join(OUT_DIR, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)

@@ -104,3 +104,18 @@ def test_wilson_interval(sg):
     assert sg.wilson_interval(7, 7)[1] == 1.0
     with pytest.raises(sg.SograndError):
         sg.wilson_interval(5, 4)
+
+
+def test_wait_limit_is_clamped(sg):
+    """The device wait limit is process state only; no GPU is touched."""
+    from sogrand_b200 import _lib
+
+    lib = _lib.load()
+    old = lib.sg_get_wait_limit()
+    assert old == 1 << 22
+    try:
+        assert lib.sg_set_wait_limit(1 << 40) == 0
+        assert lib.sg_get_wait_limit() == 1 << 22
+        assert lib.sg_set_wait_limit(5) == 0 and lib.sg_get_wait_limit() == 5
+    finally:
+        lib.sg_set_wait_limit(old)
