@@ -359,8 +359,9 @@ def main():
                "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
                "api": "sg_decode_host (host buffers, copies inside the timed region)"}
 
-    ceil = C.c_double()
-    _lib.check(lib.sg_guess_ceiling(20000, C.byref(ceil)))
+    ceil, ceil_tab = C.c_double(), C.c_double()
+    _lib.check(lib.sg_guess_ceiling(20000, 0, C.byref(ceil)))
+    _lib.check(lib.sg_guess_ceiling(20000, 1, C.byref(ceil_tab)))
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -384,7 +385,10 @@ def main():
                               "peak": ceil.value, "unit": "guess/s per GPU",
                               "frac": value * ng_per_cw / world / ceil.value,
                               "how": "sg_guess_ceiling: PM add + exp(-PM) + P_notGuess subtract per guess, "
-                                     "all SMs, measured on this GPU in this run"},
+                                     "all SMs, measured on this GPU in this run, with the decoder's correctly "
+                                     "rounded exp",
+                              "peak_table_exp": ceil_tab.value,
+                              "frac_table_exp": value * ng_per_cw / world / ceil_tab.value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": DRAM_BYTES_PER_CW[args.form] * n,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of 2368 codewords "

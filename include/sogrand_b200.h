@@ -311,9 +311,11 @@ sg_status sg_check_device(void* stream);
 /* Measured ceiling of the per-guess floating-point work on the current
  * device: one path-metric addition, one exp(-PM) and one P_notGuess
  * subtraction per guess, all SMs, no memory traffic; 2*iters guesses per
- * thread.  Synchronous.  The decoder's guesses/s divided by this is its
- * fraction of the arithmetic bound. */
-sg_status sg_guess_ceiling(unsigned long long iters, double* guesses_per_second);
+ * thread.  mode 0: with the decoder's correctly rounded exp; mode 1: with
+ * the table-driven exp of the generator (within 0.51 ulp).  Synchronous.
+ * The decoder's guesses/s divided by the mode-0 figure is its fraction of
+ * the arithmetic bound. */
+sg_status sg_guess_ceiling(unsigned long long iters, int32_t mode, double* guesses_per_second);
 
 /* The order in which a line decode tests error patterns when its
  * reliability shift is IC (the loops of sogrand_main_logic,

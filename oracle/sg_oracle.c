@@ -8,7 +8,8 @@
  *   C = SOGRAND_C/channel_sim.c
  *
  * Compile with -DSGO_TWIN=1 to evaluate exp/log with the kernel's own
- * routines (sogrand_b200/csrc/sg_math.h) instead of libm.
+ * routines (sogrand_b200/csrc/sg_crmath.h) instead of libm, and with
+ * -DSGO_CRQ=1 with the binary128-based correctly rounded ones of crq.h.
  */
 #include "sg_oracle.h"
 
@@ -26,50 +27,24 @@
 #endif
 
 #if SGO_CRQ
-/* Correctly rounded exp/log, as a checker: x87 extended precision first
- * (about 2^-62 relative error), and, when that result lies within 2^-60 of
- * the midpoint between two doubles, binary128 (libquadmath) rounded once to
- * double.  Slow and host-only; it serves to measure what a correctly
- * rounded libm changes and to check correctly rounded implementations. */
-#include <quadmath.h>
-static double crq_round(long double y, double x, int is_exp)
-{
-    double d = (double)y; /* round to nearest */
-    if (!(d == d) || d == 0.0 || d > 1.7976931348623157e308 || d < -1.7976931348623157e308)
-        return d;
-    long double diff = y - (long double)d;
-    double nb = nextafter(d, diff > 0 ? INFINITY : -INFINITY);
-    long double half = fabsl((long double)nb - (long double)d) / 2;
-    if (fabsl(fabsl(diff) - half) > ldexpl(fabsl(y), -60))
-        return d;
-    __float128 q = is_exp ? expq((__float128)x) : logq((__float128)x);
-    return (double)q;
-}
-static double ox_exp(double x)
-{
-    if (!(x <= 709.782712893384))
-        return x != x ? x : INFINITY;
-    if (x < -745.2)
-        return 0.0;
-    return crq_round(expl((long double)x), x, 1);
-}
-static double ox_log(double x)
-{
-    if (!(x > 0.0) || x > 1.7976931348623157e308)
-        return log(x);
-    return crq_round(logl((long double)x), x, 0);
-}
+/* correctly rounded through extended and binary128 precision (crq.h) */
+#include "crq.h"
+static double ox_exp(double x) { return crq_exp(x); }
+static double ox_log(double x) { return crq_log(x); }
 static double ox_pow2_neg(double s) { return pow(2.0, -s); }
 #elif SGO_TWIN
-#include "../sogrand_b200/csrc/sg_math.h"
+/* the decoder's own exp/log: correctly rounded (sg_crmath.h), or, built
+ * with SG_CR_MATH=0, the table-driven routines of sg_math.h -- as the
+ * kernel is built */
+#include "../sogrand_b200/csrc/sg_crmath.h"
 static const double k_etab[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
 static const double k_ltab[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
-#if SGO_TWIN_ONLY == 1 /* diagnostic: only exp from sg_math.h */
-static double ox_exp(double x) { return sg_exp(x, k_etab); }
-static double ox_log(double x) { return log(x); }
-#elif SGO_TWIN_ONLY == 2 /* diagnostic: only log from sg_math.h */
-static double ox_exp(double x) { return exp(x); }
-static double ox_log(double x) { return sg_log(x, k_ltab); }
+#ifndef SG_CR_MATH
+#define SG_CR_MATH 1
+#endif
+#if SG_CR_MATH
+static double ox_exp(double x) { return sg_exp_cr(x, k_etab); }
+static double ox_log(double x) { return sg_log_cr(x, k_ltab); }
 #else
 static double ox_exp(double x) { return sg_exp(x, k_etab); }
 static double ox_log(double x) { return sg_log(x, k_ltab); }
@@ -447,6 +422,16 @@ size_t sgo_pattern_order(int32_t ic, uint32_t* out, size_t cap)
 
 double sgo_exp(double x) { return ox_exp(x); }
 double sgo_log(double x) { return ox_log(x); }
+
+#if SGO_TWIN
+/* Diagnostics of the decoder's math (twin build): the correctly rounded
+ * routines' slow paths on their own (finite x; log: x > 0), and the
+ * table-driven routines the input generator uses. */
+double sgo_exp_cr_slow(double x) { return sg_exp_cr_slow(x, k_etab); }
+double sgo_log_cr_slow(double x) { return sg_log_cr_slow(x, k_ltab); }
+double sgo_exp_tab(double x) { return sg_exp(x, k_etab); }
+double sgo_log_tab(double x) { return sg_log(x, k_ltab); }
+#endif
 
 static void bitso_state(const double llr[SGO_N], int L, uint64_t Tmax, double thres, sgo_line_out* out,
                         line_state* sp);

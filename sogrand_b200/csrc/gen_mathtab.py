@@ -14,6 +14,10 @@ the mathematics with mpmath at 256-bit precision and rounded to nearest:
         two subintervals that touch 1.0, so log(x) near 1 has no cancellation),
         and -log(c_j) is stored as a double-double (hi, lo).
 
+The correctly rounded routines of sg_crmath.h reuse both tables; their
+extra constants (range limits, a three-part ln2/128, Taylor coefficients in
+double-double) are derived the same way.
+
 Run:  python gen_mathtab.py > sg_mathtab.h
 """
 import struct
@@ -112,7 +116,67 @@ def main():
             h, l = dd(-mp.log(mp.mpf(cj)))
         rows.append("  %s, %s, %s" % (hexd(cj), hexd(h), hexd(l)))
     w(", \\\n".join(rows) + " \\\n}")
+
+    # ---- correctly rounded exp/log (sg_crmath.h), same tables as above
+    w("/* correctly rounded exp/log (sg_crmath.h) */")
+    w("#define SG_CR_EXP_XMAX %s  /* largest x with RN(exp(x)) finite */" % hexd(EXP_XMAX))
+    w("#define SG_CR_EXP_XMIN %s  /* smallest x with RN(exp(x)) > 0 */" % hexd(EXP_XMIN))
+    # ln2/N = C1 + C2 + C3: C1 and C2 keep 35 significant bits (k*C1, k*C2
+    # exact for |k| < 2^18), C3 the rounded rest
+    c = ln2 / N
+    e1 = int(mp.floor(mp.log(c, 2)))
+    q1 = mp.mpf(2) ** (e1 - 34)
+    C1 = mp.floor(c / q1) * q1
+    rest = c - C1
+    e2 = int(mp.floor(mp.log(rest, 2)))
+    q2 = mp.mpf(2) ** (e2 - 34)
+    C2 = mp.floor(rest / q2) * q2
+    C3 = rn(rest - C2)
+    w("#define SG_CR_EXP_C1 %s" % hexd(float(C1)))
+    w("#define SG_CR_EXP_C2 %s" % hexd(float(C2)))
+    w("#define SG_CR_EXP_C3 %s" % hexd(C3))
+    # 1/n!: double-double for n = 2..5, double for n = 6..11
+    for n in range(2, 12):
+        v = mp.mpf(1) / mp.factorial(n)
+        if n <= 5:
+            h, l = dd(v)
+            w("#define SG_CR_EXP_F%d_HI %s" % (n, hexd(h)))
+            w("#define SG_CR_EXP_F%d_LO %s" % (n, hexd(l)))
+        else:
+            w("#define SG_CR_EXP_F%d %s" % (n, hexd(rn(v))))
+    # ln2 = SG_LOG_LN2_HI + SG_LOG_LN2_LO + SG_CR_LOG_LN2_LO2
+    w("#define SG_CR_LOG_LN2_LO2 %s" % hexd(rn(ln2 - mp.mpf(l2hi) - mp.mpf(l2lo))))
+    # (-1)^(n+1)/n: double for n = 2..17, double-double too for n = 2..9
+    for n in range(2, 18):
+        v = mp.mpf((-1) ** (n + 1)) / n
+        if n <= 9:
+            h, l = dd(v)
+            w("#define SG_CR_LOG_G%d_HI %s" % (n, hexd(h)))
+            w("#define SG_CR_LOG_G%d_LO %s" % (n, hexd(l)))
+        w("#define SG_CR_LOG_G%d %s" % (n, hexd(rn(v))))
     print("\n".join(out))
+
+
+def _exp_limits():
+    """Largest x with RN(exp(x)) finite and smallest x with RN(exp(x)) > 0."""
+    dmax = from_bits(0x7FEFFFFFFFFFFFFF)
+    top = mp.mpf(dmax) + mp.mpf(2) ** (1023 - 53)
+    x = float(mp.log(top))
+    while mp.exp(mp.mpf(x)) >= top:
+        x = from_bits(bits(x) - 1)
+    while mp.exp(mp.mpf(from_bits(bits(x) + 1))) < top:
+        x = from_bits(bits(x) + 1)
+    xmax = x
+    bot = mp.mpf(2) ** -1075
+    x = float(mp.log(bot))
+    while mp.exp(mp.mpf(x)) <= bot:
+        x = from_bits(bits(x) - 1)
+    while mp.exp(mp.mpf(from_bits(bits(x) + 1))) > bot:
+        x = from_bits(bits(x) + 1)
+    return xmax, x
+
+
+EXP_XMAX, EXP_XMIN = _exp_limits()
 
 
 if __name__ == "__main__":

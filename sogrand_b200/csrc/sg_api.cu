@@ -113,7 +113,7 @@ template <int NW, bool LCH_SMEM>
 struct SgCwSmem {
     alignas(16) double lch[LCH_SMEM ? SG_CUBE : 2]; /* bulk-copy destination */
     double le[SG_CUBE];
-    alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by sg_exp_neg */
+    alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by the exp routines */
     alignas(16) double ltab[SG_LOG_TAB_LEN];
     SgWarpScratch ws[NW];
     uint16_t hdw[256];
@@ -590,10 +590,12 @@ __global__ void sg_enum_build_kernel(uint32_t* out, unsigned int* ok)
 }
 
 /* Ceiling of the per-guess floating-point work: each thread evaluates, per
- * iteration, one path-metric addition, exp(-PM) (sg_exp_neg, the guess
- * loop's routine) and one P_notGuess subtraction, with no memory traffic
- * beyond the shared exp table.  guesses/s of this kernel over all SMs bounds
- * what any decoder with the reference's per-guess arithmetic can reach. */
+ * iteration, one path-metric addition, exp(-PM) and one P_notGuess
+ * subtraction, with no memory traffic beyond the shared exp table.
+ * guesses/s of this kernel over all SMs bounds what any decoder with the
+ * reference's per-guess arithmetic can reach.  CR: the correctly rounded
+ * exp; otherwise the table-driven sg_exp_neg. */
+template <bool CR>
 __global__ void __launch_bounds__(256) sg_guess_ceiling_kernel(unsigned long long iters, double* sink)
 {
     __shared__ alignas(16) double etab[SG_EXP_TAB_LEN];
@@ -604,8 +606,8 @@ __global__ void __launch_bounds__(256) sg_guess_ceiling_kernel(unsigned long lon
     for (unsigned long long k = 0; k < iters; k++) {
         pm0 = __dadd_rn(pm0, 1.1e-5);
         pm1 = __dadd_rn(pm1, 1.3e-5);
-        acc0 = __dsub_rn(acc0, sg_exp_neg(-pm0, etab));
-        acc1 = __dsub_rn(acc1, sg_exp_neg(-pm1, etab));
+        acc0 = __dsub_rn(acc0, CR ? sg_exp_cr_neg(-pm0, etab) : sg_exp_neg(-pm0, etab));
+        acc1 = __dsub_rn(acc1, CR ? sg_exp_cr_neg(-pm1, etab) : sg_exp_neg(-pm1, etab));
     }
     if (acc0 + acc1 == 12345.0)
         sink[blockIdx.x] = acc0;
@@ -1482,10 +1484,12 @@ sg_status sg_batch_set_variant(int v)
 
 int sg_batch_get_variant(void) { return g_pvariant; }
 
-sg_status sg_guess_ceiling(unsigned long long iters, double* guesses_per_second)
+sg_status sg_guess_ceiling(unsigned long long iters, int32_t mode, double* guesses_per_second)
 {
-    if (!guesses_per_second || iters == 0)
-        return fail(SG_ERR_ARG, "need iters > 0 and an output pointer");
+    if (!guesses_per_second || iters == 0 || (mode != 0 && mode != 1))
+        return fail(SG_ERR_ARG, "need iters > 0, mode 0 or 1 and an output pointer");
+    void (*kern)(unsigned long long, double*) =
+        mode == 0 ? sg_guess_ceiling_kernel<true> : sg_guess_ceiling_kernel<false>;
     DevCtx* c = nullptr;
     sg_status s = get_ctx(&c);
     if (s != SG_OK)
@@ -1494,9 +1498,9 @@ sg_status sg_guess_ceiling(unsigned long long iters, double* guesses_per_second)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     SG_CUDA(cudaEventCreate(&e0));
     SG_CUDA(cudaEventCreate(&e1));
-    sg_guess_ceiling_kernel<<<blocks, 256>>>(iters / 8 + 1, c->err_sink); /* warm-up */
+    kern<<<blocks, 256>>>(iters / 8 + 1, c->err_sink); /* warm-up */
     SG_CUDA(cudaEventRecord(e0));
-    sg_guess_ceiling_kernel<<<blocks, 256>>>(iters, c->err_sink);
+    kern<<<blocks, 256>>>(iters, c->err_sink);
     SG_CUDA(cudaEventRecord(e1));
     SG_CUDA(cudaEventSynchronize(e1));
     float ms = 0;

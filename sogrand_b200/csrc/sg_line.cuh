@@ -40,8 +40,37 @@
 #pragma once
 #include <stddef.h>
 #include <stdint.h>
+#include "sg_crmath.h"
 #include "sg_enum.h"
 #include "sg_math.h"
+
+/* The decoder's exp and log.  SG_CR_MATH = 1 (default): correctly rounded
+ * (sg_crmath.h), so that results equal the reference's under any correctly
+ * rounded libm; 0: the table-driven routines of sg_math.h (within 0.51 ulp),
+ * kept for comparison. */
+#ifndef SG_CR_MATH
+#define SG_CR_MATH 1
+#endif
+/* SG_EXP_HYBRID (with SG_CR_MATH): the guess loop first evaluates the
+ * table-driven exp (within 0.51 ulp, so the correctly rounded value is the
+ * same double or a neighbour) and keeps it wherever that cannot change the
+ * result -- a step that P_notGuess crosses by the exact integer sum, where
+ * only round(e / ulp(P)) enters and every term is at least 2^-51 of its own
+ * magnitude away from a rounding tie; every other step (codewords, binade
+ * crossings, near-ties) re-evaluates the correctly rounded exp of all its
+ * patterns and uses those throughout. */
+#ifndef SG_EXP_HYBRID
+#define SG_EXP_HYBRID SG_CR_MATH
+#endif
+#if SG_CR_MATH
+#define SG_EXP(x, t) sg_exp_cr(x, t)
+#define SG_EXP_NEG(x, t) sg_exp_cr_neg(x, t)
+#define SG_LOG(x, t) sg_log_cr(x, t)
+#else
+#define SG_EXP(x, t) sg_exp(x, t)
+#define SG_EXP_NEG(x, t) sg_exp_neg(x, t)
+#define SG_LOG(x, t) sg_log(x, t)
+#endif
 
 #define SG_FULL 0xffffffffu
 
@@ -272,10 +301,10 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
      * for the sorted PM increments below */
     const double a_all = __shfl_sync(SG_FULL, a, lane & 15);
     const double xj = act ? -a_all : a_all;
-    const double ex = sg_exp(xj, etab);
+    const double ex = SG_EXP(xj, etab);
     /* JacLog(xj) = xj if xj > 50, 0 if xj < -50, else log(1 + e^xj) (:762),
      * with its exp kept */
-    const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : sg_log(1.0 + ex, ltab));
+    const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : SG_LOG(1.0 + ex, ltab));
     const double jn = act ? jl : 0.0;
     {
         /* the soft output's exp(LLR) of position p is this exp of lane p + 16
@@ -458,8 +487,9 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             break;
         }
         /* G patterns per lane: lane j of half h tests pattern base + 32h + j */
+        constexpr bool HYB = SG_EXP_HYBRID && !ADJ;
         uint32_t ent[G];
-        double e[G];
+        double e[G], pmv[G];
         uint32_t hits[G];
         int nv[G];
         int nvt = 0; /* valid patterns of the step, in order */
@@ -512,7 +542,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                     rest &= rest - 1u;
                 }
             }
-            e[h] = sg_exp_neg(-pm, etab);
+            pmv[h] = pm;
+            e[h] = HYB ? sg_exp_neg(-pm, etab) : SG_EXP_NEG(-pm, etab);
             hits[h] = __ballot_sync(SG_FULL, syn == 0u) & (nv[h] >= 32 ? SG_FULL : ((1u << nv[h]) - 1u));
             nvt += nv[h];
         }
@@ -537,7 +568,11 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                 const double q = lane < nv[h] ? __dmul_rn(e[h], iu) : 0.0;
                 const double t = __dadd_rn(q, 0x1p52);
                 const double d = __dsub_rn(t, 0x1p52);
-                bad |= !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
+                /* a tie (or, with the table-driven exp, anything within
+                 * q 2^-51 >= 2 ulp(q) of one) goes to the general case */
+                bad |= !(q < 0x1p52) ||
+                       (HYB ? fabs(__dsub_rn(q, d)) >= __dsub_rn(0.5, __dmul_rn(q, 0x1p-51))
+                            : fabs(__dsub_rn(q, d)) == 0.5);
                 const uint64_t tb = sg_bits(t);
                 slo += (uint32_t)tb & 0x3ffffffu;
                 shi += (uint32_t)(tb >> 26) & 0x3ffffffu;
@@ -560,6 +595,11 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
         /* general case, one half after the other */
         if (!stepped) {
+            if (HYB) {
+#pragma unroll
+                for (int h = 0; h < G; h++)
+                    e[h] = SG_EXP_NEG(-pmv[h], etab);
+            }
 #pragma unroll
             for (int h = 0; h < G; h++) {
                 if (done)
@@ -646,7 +686,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         }
         p0 = __dadd_rn(p0, __dmul_rn(pnlc, pp0));
         p1 = __dadd_rn(p1, __dmul_rn(pnlc, pp1));
-        const double lg = sg_log(fmax(act ? p0 : p1, 1e-40), ltab);
+        const double lg = SG_LOG(fmax(act ? p0 : p1, 1e-40), ltab);
         lapp = __dsub_rn(lg, __shfl_sync(SG_FULL, lg, (lane & 15) + 16));
         le = __dsub_rn(lapp, x);
     }

@@ -285,3 +285,56 @@
   0x1.77908119ac60dp-1, 0x1.3d54fa5c1f710p-2, 0x1.53668e578d9cdp-58, \
   0x1.756cac201756dp-1, 0x1.432ef2a04e813p-2, -0x1.83262e2b59206p-57 \
 }
+/* correctly rounded exp/log (sg_crmath.h) */
+#define SG_CR_EXP_XMAX 0x1.62e42fefa39efp+9  /* largest x with RN(exp(x)) finite */
+#define SG_CR_EXP_XMIN -0x1.74910d52d3051p+9  /* smallest x with RN(exp(x)) > 0 */
+#define SG_CR_EXP_C1 0x1.62e42fef80000p-8
+#define SG_CR_EXP_C2 0x1.1cf79abc80000p-43
+#define SG_CR_EXP_C3 0x1.e3b39803f2f6bp-79
+#define SG_CR_EXP_F2_HI 0x1.0000000000000p-1
+#define SG_CR_EXP_F2_LO 0x0.0p+0
+#define SG_CR_EXP_F3_HI 0x1.5555555555555p-3
+#define SG_CR_EXP_F3_LO 0x1.5555555555555p-57
+#define SG_CR_EXP_F4_HI 0x1.5555555555555p-5
+#define SG_CR_EXP_F4_LO 0x1.5555555555555p-59
+#define SG_CR_EXP_F5_HI 0x1.1111111111111p-7
+#define SG_CR_EXP_F5_LO 0x1.1111111111111p-63
+#define SG_CR_EXP_F6 0x1.6c16c16c16c17p-10
+#define SG_CR_EXP_F7 0x1.a01a01a01a01ap-13
+#define SG_CR_EXP_F8 0x1.a01a01a01a01ap-16
+#define SG_CR_EXP_F9 0x1.71de3a556c734p-19
+#define SG_CR_EXP_F10 0x1.27e4fb7789f5cp-22
+#define SG_CR_EXP_F11 0x1.ae64567f544e4p-26
+#define SG_CR_LOG_LN2_LO2 0x1.f97b57a079a19p-103
+#define SG_CR_LOG_G2_HI -0x1.0000000000000p-1
+#define SG_CR_LOG_G2_LO 0x0.0p+0
+#define SG_CR_LOG_G2 -0x1.0000000000000p-1
+#define SG_CR_LOG_G3_HI 0x1.5555555555555p-2
+#define SG_CR_LOG_G3_LO 0x1.5555555555555p-56
+#define SG_CR_LOG_G3 0x1.5555555555555p-2
+#define SG_CR_LOG_G4_HI -0x1.0000000000000p-2
+#define SG_CR_LOG_G4_LO 0x0.0p+0
+#define SG_CR_LOG_G4 -0x1.0000000000000p-2
+#define SG_CR_LOG_G5_HI 0x1.999999999999ap-3
+#define SG_CR_LOG_G5_LO -0x1.999999999999ap-57
+#define SG_CR_LOG_G5 0x1.999999999999ap-3
+#define SG_CR_LOG_G6_HI -0x1.5555555555555p-3
+#define SG_CR_LOG_G6_LO -0x1.5555555555555p-57
+#define SG_CR_LOG_G6 -0x1.5555555555555p-3
+#define SG_CR_LOG_G7_HI 0x1.2492492492492p-3
+#define SG_CR_LOG_G7_LO 0x1.2492492492492p-57
+#define SG_CR_LOG_G7 0x1.2492492492492p-3
+#define SG_CR_LOG_G8_HI -0x1.0000000000000p-3
+#define SG_CR_LOG_G8_LO 0x0.0p+0
+#define SG_CR_LOG_G8 -0x1.0000000000000p-3
+#define SG_CR_LOG_G9_HI 0x1.c71c71c71c71cp-4
+#define SG_CR_LOG_G9_LO 0x1.c71c71c71c71cp-58
+#define SG_CR_LOG_G9 0x1.c71c71c71c71cp-4
+#define SG_CR_LOG_G10 -0x1.999999999999ap-4
+#define SG_CR_LOG_G11 0x1.745d1745d1746p-4
+#define SG_CR_LOG_G12 -0x1.5555555555555p-4
+#define SG_CR_LOG_G13 0x1.3b13b13b13b14p-4
+#define SG_CR_LOG_G14 -0x1.2492492492492p-4
+#define SG_CR_LOG_G15 0x1.1111111111111p-4
+#define SG_CR_LOG_G16 -0x1.0000000000000p-4
+#define SG_CR_LOG_G17 0x1.e1e1e1e1e1e1ep-5

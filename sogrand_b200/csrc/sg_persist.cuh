@@ -36,7 +36,7 @@ struct SgSlot {
 template <int NW, int C>
 struct SgPersistSmem {
     SgSlot slot[C];
-    alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by sg_exp_neg */
+    alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by the exp routines */
     alignas(16) double ltab[SG_LOG_TAB_LEN];
     SgWarpScratch ws[NW];
 };

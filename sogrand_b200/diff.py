@@ -28,6 +28,23 @@ def _params(alpha_np, imax: int, L: int):
     return sg.params(L=L, Imax=imax, alpha=a)
 
 
+def _check_cube(llr, name="llr"):
+    """The C ABI reads llr as contiguous float64 [n, 4096] device memory."""
+    import torch
+
+    if not (llr.is_cuda and llr.dtype == torch.float64 and llr.is_contiguous() and llr.dim() == 2
+            and llr.shape[1] == 4096):
+        raise ValueError(f"{name} must be a contiguous CUDA float64 tensor of shape [n, 4096]")
+
+
+def _check_bits(code_bits, n):
+    import torch
+
+    if not (code_bits.is_cuda and code_bits.dtype == torch.uint8 and code_bits.is_contiguous()
+            and tuple(code_bits.shape) == (n, 4096)):
+        raise ValueError("code_bits must be a contiguous CUDA uint8 tensor of shape [n, 4096]")
+
+
 def _torch_fn():
     import torch
 
@@ -37,7 +54,9 @@ def _torch_fn():
             import sogrand_b200 as sg
 
             lib = _lib.load()
+            _check_cube(llr)
             n = llr.shape[0]
+            _check_bits(code_bits, n)
             nph = 3 * imax
             dev = llr.device
             p = _params(alpha.detach().cpu().numpy(), imax, L)
@@ -90,7 +109,8 @@ def decode_bce(alpha, llr, code_bits, imax: int = 30, L: int = 3):
     global _FN
     if _FN is None:
         _FN = _torch_fn()
-    return _FN.apply(alpha, llr, code_bits.contiguous(), imax, L)
+    # contiguous() keeps the autograd path to a non-contiguous llr
+    return _FN.apply(alpha, llr.contiguous(), code_bits.contiguous(), imax, L)
 
 
 def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False):
@@ -99,7 +119,9 @@ def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False):
 
     import sogrand_b200 as sg
 
+    _check_cube(llr)
     n = llr.shape[0]
+    _check_bits(code_bits, n)
     nph = 3 * p.Imax
     dev = llr.device
     loss = torch.empty(n, dtype=torch.float64, device=dev)
@@ -118,6 +140,7 @@ def forward_raw(llr, p):
 
     import sogrand_b200 as sg
 
+    _check_cube(llr)
     n = llr.shape[0]
     dev = llr.device
     ckpt = torch.empty((n, 3 * p.Imax, sg.SG_CUBE), dtype=torch.float64, device=dev)

@@ -34,10 +34,15 @@ def kat():
 
 @pytest.fixture(scope="session")
 def oracle_paths():
-    """The CPU checkers (built from oracle/ if missing)."""
+    """The CPU checkers (built from oracle/ if missing).  "crq" (the
+    binary128 checker, needs libquadmath) is None where it cannot be built."""
     d = os.path.join(ROOT, "oracle")
     _ensure_built(d, ["libsg_oracle.so", "libsg_oracle_twin.so"])
-    return {"libm": os.path.join(d, "libsg_oracle.so"), "twin": os.path.join(d, "libsg_oracle_twin.so")}
+    crq = os.path.join(d, "libsg_oracle_crq.so")
+    if not os.path.exists(crq):
+        subprocess.run(["make", "-C", d, "crq"], capture_output=True)
+    return {"libm": os.path.join(d, "libsg_oracle.so"), "twin": os.path.join(d, "libsg_oracle_twin.so"),
+            "crq": crq if os.path.exists(crq) else None}
 
 
 @pytest.fixture(scope="session")

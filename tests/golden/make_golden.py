@@ -9,13 +9,23 @@ the reference is available, not on the GPU machine):
 Inputs are the seeded synthetic channel outputs of sogrand_b200.gen_llr
 (regenerated bit-identically at test time and checked against the SHA-256
 recorded here).  Expected outputs come from
-  - the unmodified reference SOGRAND_C/cubic_decoder_final.c, through
-    oracle/_ref/libsgref.so (reference functions + a per-codeword driver) and,
-    for the main fixture, through the unmodified flow binary
-    oracle/_ref/cubic_decoder_final (decoded file and printed averages);
-  - the twin oracle oracle/libsg_oracle_twin.so: the same algorithm with the
-    decoder's own exp/log, whose soft values the CUDA kernel must reproduce
-    bit for bit.
+  - "ref": the unmodified reference SOGRAND_C/cubic_decoder_final.c with the
+    system libm (glibc), through oracle/_ref/libsgref.so (reference functions
+    + a per-codeword driver) and, for the main fixture, through the
+    unmodified flow binary oracle/_ref/cubic_decoder_final (decoded file and
+    printed averages);
+  - "ref_cr": the same unmodified source compiled against a correctly
+    rounded exp/log (oracle/_ref/libsgref_cr.so, oracle/cr_libm.c) -- the
+    decoder's bit-exact target, soft values included;
+  - "twin": the oracle restatement with the decoder's own exp/log
+    (oracle/libsg_oracle_twin.so); the generator checks that it equals
+    "ref_cr" in every recorded value where the reference is defined.
+"ref" and "ref_cr" differ only where glibc's exp/log are not correctly
+rounded; the count of codewords where that moves a discrete result is
+recorded per set.  Per-line known answers come from both reference builds,
+with and without a Tmax cap; a line that lists no codeword under the cap
+makes the reference read an uninitialised list size, so only its N_guess is
+recorded there.
 Writes tests/golden/golden.json and tests/golden/kat_lines.npz.
 """
 from __future__ import annotations
@@ -36,6 +46,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libsgref.so")
+REF_CR_SO = os.path.join(ROOT, "oracle", "_ref", "libsgref_cr.so")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder_final")
 TWIN_SO = os.path.join(ROOT, "oracle", "libsg_oracle_twin.so")
 OUT_DIR = os.path.join(ROOT, "tests", "golden")
@@ -82,9 +93,10 @@ class Stats(C.Structure):
 
 def ref_one(args):
     """Reference decode of one codeword -> (bits, iters, ng, ngp, conv, lapp
-    sha, line decodes that read the reference's uninitialised list size)."""
-    llr, tmax = args
-    lib = C.CDLL(REF_SO)
+    sha, line decodes that read the reference's uninitialised list size).
+    args: (llr, Tmax[, reference library])."""
+    llr, tmax = args[:2]
+    lib = C.CDLL(args[2] if len(args) > 2 else REF_SO)
     dp = np.ctypeslib.ndpointer(np.float64, flags="C")
     u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
     u64 = np.ctypeslib.ndpointer(np.uint64, flags="C")
@@ -157,7 +169,7 @@ def kat_lines(rng, cubes):
 
 
 def main():
-    for f in (REF_SO, REF_BIN, TWIN_SO):
+    for f in (REF_SO, REF_CR_SO, REF_BIN, TWIN_SO):
         if not os.path.exists(f):
             sys.exit(f"missing {f}: run `make -C oracle all ref` first")
     golden = {"generator": "sogrand_b200.gen_llr (splitmix counter RNG, polar Gaussian, sg_log)",
@@ -169,7 +181,11 @@ def main():
             info, llr = gen(seed, n, snr)
             jobs = [(llr[i], tmax) for i in range(n)]
             ref = pool.map(ref_one, jobs)
+            ref_cr = pool.map(ref_one, [(llr[i], tmax, REF_CR_SO) for i in range(n)])
             twin = pool.map(twin_one, jobs)
+            for i in range(n):  # the restatement equals the reference under a correctly rounded libm
+                if ref_cr[i][6] == 0:
+                    assert twin[i][:6] == ref_cr[i][:6], (name, i, twin[i][:5], ref_cr[i][:5])
             entry = {
                 "seed": seed, "n_cw": n, "ebn0_db": snr, "Tmax": tmax,
                 "llr_sha256": sha(llr.tobytes()), "info_sha256": sha(info.tobytes()),
@@ -177,17 +193,21 @@ def main():
                         "ng": [r[2] for r in ref], "ng_p": [r[3] for r in ref],
                         "converged": [r[4] for r in ref], "lapp_sha256": [r[5] for r in ref],
                         "undefined_lines": [r[6] for r in ref]},
+                "ref_cr": {"bits": [r[0] for r in ref_cr], "iterations": [r[1] for r in ref_cr],
+                           "ng": [r[2] for r in ref_cr], "ng_p": [r[3] for r in ref_cr],
+                           "converged": [r[4] for r in ref_cr], "lapp_sha256": [r[5] for r in ref_cr],
+                           "undefined_lines": [r[6] for r in ref_cr]},
                 "twin": {"bits": [r[0] for r in twin], "iterations": [r[1] for r in twin],
                          "ng": [r[2] for r in twin], "ng_p": [r[3] for r in twin],
                          "converged": [r[4] for r in twin], "lapp_sha256": [r[5] for r in twin]},
             }
-            mism = sum(1 for a, b in zip(ref, twin) if a[:5] != b[:5])
-            entry["ref_vs_twin_discrete_mismatches"] = mism
+            mism = sum(1 for a, b in zip(ref, ref_cr) if a[:5] != b[:5])
+            entry["glibc_vs_cr_mismatches"] = mism
             ber = np.mean(np.unpackbits(np.frombuffer(b"".join(bytes.fromhex(r[0]) for r in ref), np.uint8))
                           != np.unpackbits(info.ravel()))
             entry["ref_ber"] = float(ber)
             golden["sets"][name] = entry
-            print(f"{name}: {n} cw, ref-vs-twin discrete mismatches {mism}, BER {ber:.3g}, "
+            print(f"{name}: {n} cw, glibc-vs-correctly-rounded reference mismatches {mism}, BER {ber:.3g}, "
                   f"avg it {np.mean([r[1] for r in ref]):.2f}, {time.time() - t0:.0f}s", flush=True)
 
     # the unmodified flow binary on the main fixture: decoded file + averages
@@ -211,14 +231,17 @@ def main():
     rng = np.random.default_rng(7)
     _, cubes = gen(SETS[1][1], 8, SETS[1][3])
     lines = kat_lines(rng, cubes)
-    ref = C.CDLL(REF_SO)
     dp = np.ctypeslib.ndpointer(np.float64, flags="C")
-    ref.sgref_bitso.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, dp, dp, C.POINTER(C.c_int)]
-    ref.sgref_line_undefined.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, C.POINTER(C.c_double)]
     kat = {"llr": lines}
     runs = [(3, UINT64_MAX, "L3"), (1, UINT64_MAX, "L1"), (4, UINT64_MAX, "L4")]
     runs += [(3, t, f"T{t}") for t in KAT_TMAX]
-    for L, tmax, tag in runs:
+    # tag "<run>_..." from the reference with glibc, "<run>_cr_..." from it
+    # under a correctly rounded exp/log
+    runs = [(L, t, tag, REF_SO) for L, t, tag in runs] + [(L, t, tag + "_cr", REF_CR_SO) for L, t, tag in runs]
+    for L, tmax, tag, so in runs:
+        ref = C.CDLL(so)
+        ref.sgref_bitso.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, dp, dp, C.POINTER(C.c_int)]
+        ref.sgref_line_undefined.argtypes = [dp, C.c_int, C.c_uint64, C.c_double, C.POINTER(C.c_double)]
         lapp = np.zeros_like(lines)
         le = np.zeros_like(lines)
         ng = np.zeros(len(lines), np.int32)

@@ -1,21 +1,26 @@
-"""Large reference-pinned fixtures and the reference-vs-restatement survey.
+"""Large reference-pinned fixtures and the glibc / correctly-rounded survey.
 
 Run from the repository root where the reference sources are available
-(after `make -C oracle all crq ref && make -C sogrand_b200/csrc`):
+(after `make -C oracle all crq tab ref REF=<reference root>` and
+`make -C sogrand_b200/csrc`):
 
-    python tests/golden/make_golden_large.py [--procs N]
+    python tests/golden/make_golden_large.py [--procs N] [--kinds ref,ref_cr,tab]
 
 For each set below, every codeword is decoded by
-  ref   the unmodified reference (oracle/_ref/libsgref.so: the reference's
-        SOGRAND_bitSO / early_termination / hard_decision, glibc exp/log),
-  twin  the restatement with the decoder's own exp/log (libsg_oracle_twin.so),
-  crq   the restatement with correctly rounded exp/log (libsg_oracle_crq.so),
-and the discrete results (decoded bits, iterations, NG, NG_p, converged) are
-written to tests/golden/golden_large.npz.  The restatements differ from the
-reference only through the last bits of exp/log, so the count of codewords
-whose statistics differ measures what each exp/log choice costs in
-reference parity.  Inputs are sogrand_b200.gen_llr's seeded channel outputs,
-checked at test time by SHA-256.
+  ref     the unmodified reference (oracle/_ref/libsgref.so: the reference's
+          SOGRAND_bitSO / early_termination / hard_decision, glibc exp/log),
+  ref_cr  the same unmodified source under a correctly rounded exp/log
+          (oracle/_ref/libsgref_cr.so) -- the decoder's exact target,
+  tab     the restatement with the table-driven exp/log of sg_math.h
+          (within 0.51 ulp, not correctly rounded; libsg_oracle_tab.so),
+and the discrete results (decoded bits, iterations, NG, NG_p, converged)
+are written to tests/golden/golden_large.npz.  ref and ref_cr differ only
+through glibc's misrounded last bits, tab only through its own, so the count
+of codewords whose results differ from ref measures what each exp/log
+choice costs in parity with the glibc-linked reference.  Results already in
+the output file for the same inputs (same LLR SHA-256) are reused for kinds
+not listed in --kinds.  Inputs are sogrand_b200.gen_llr's seeded channel
+outputs, checked at test time by SHA-256.
 """
 from __future__ import annotations
 
@@ -35,12 +40,13 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 LIBS = {
     "ref": os.path.join(ROOT, "oracle", "_ref", "libsgref.so"),
-    "twin": os.path.join(ROOT, "oracle", "libsg_oracle_twin.so"),
-    "crq": os.path.join(ROOT, "oracle", "libsg_oracle_crq.so"),
+    "ref_cr": os.path.join(ROOT, "oracle", "_ref", "libsgref_cr.so"),
+    "tab": os.path.join(ROOT, "oracle", "libsg_oracle_tab.so"),
 }
 OUT = os.path.join(ROOT, "tests", "golden", "golden_large.npz")
 UINT64_MAX = (1 << 64) - 1
 THRES = 1.0 - 1e-5
+FIELDS = ("iterations", "ng", "ng_p", "converged")
 
 # (name, seed, n_cw, Eb/N0 dB)
 SETS = [
@@ -53,10 +59,10 @@ _cache: dict = {}
 
 def _decode(kind, llr):
     """One codeword -> (bits[64] u8, iterations, ng, ng_p, converged)."""
-    if kind == "ref":
-        lib = _cache.get("ref")
+    if kind in ("ref", "ref_cr"):
+        lib = _cache.get(kind)
         if lib is None:
-            lib = _cache["ref"] = C.CDLL(LIBS["ref"])
+            lib = _cache[kind] = C.CDLL(LIBS[kind])
             dp = np.ctypeslib.ndpointer(np.float64, flags="C")
             u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
             u64 = np.ctypeslib.ndpointer(np.uint64, flags="C")
@@ -89,13 +95,17 @@ def _job(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--procs", type=int, default=max(1, (os.cpu_count() or 2) - 1))
+    ap.add_argument("--kinds", default="ref,ref_cr,tab")
     ap.add_argument("--n-cw", type=int, default=0, help="override the codewords per set (testing the script)")
+    ap.add_argument("--out", default=OUT)
     args = ap.parse_args()
-    for f in LIBS.values():
-        if not os.path.exists(f):
-            sys.exit(f"missing {f}: run `make -C oracle all crq ref` first")
+    kinds = args.kinds.split(",")
+    for k in kinds:
+        if not os.path.exists(LIBS[k]):
+            sys.exit(f"missing {LIBS[k]}: run `make -C oracle all crq tab ref REF=...` first")
     import sogrand_b200 as sg
 
+    old = dict(np.load(args.out)) if os.path.exists(args.out) else {}
     out = {}
     t0 = time.time()
     ctx = mp.get_context("spawn")
@@ -103,36 +113,47 @@ def main():
         for name, seed, n, snr in SETS:
             n = args.n_cw or n
             info, llr = sg.gen_llr(seed, 0, n, ebn0_db=snr)
+            sha = hashlib.sha256(llr.tobytes()).hexdigest()
             out[f"{name}/meta"] = np.array([seed, n], np.int64)
             out[f"{name}/ebn0_db"] = np.array(snr)
-            out[f"{name}/llr_sha256"] = np.array(hashlib.sha256(llr.tobytes()).hexdigest())
+            out[f"{name}/llr_sha256"] = np.array(sha)
             out[f"{name}/info_sha256"] = np.array(hashlib.sha256(info.tobytes()).hexdigest())
-            for kind in LIBS:
+            same_inputs = str(old.get(f"{name}/llr_sha256", "")) == sha
+            full = {}
+            for kind in ("ref", "ref_cr", "tab"):
+                if kind not in kinds:
+                    if same_inputs and f"{name}/{kind}_ng" in old:
+                        bits = old[f"{name}/ref_bits"].copy()
+                        if kind != "ref":
+                            bits[old[f"{name}/{kind}_bits_diff_idx"]] = old[f"{name}/{kind}_bits_diff"]
+                        full[kind] = {"bits": bits, **{f: old[f"{name}/{kind}_{f}"] for f in FIELDS}}
+                    continue
                 res = pool.map(_job, [(kind, llr[i]) for i in range(n)], chunksize=4)
-                out[f"{name}/{kind}_bits"] = np.stack([r[0] for r in res]).astype(np.uint8)
-                out[f"{name}/{kind}_iterations"] = np.array([r[1] for r in res])
-                out[f"{name}/{kind}_ng"] = np.array([r[2] for r in res], np.uint64)
-                out[f"{name}/{kind}_ng_p"] = np.array([r[3] for r in res], np.uint64)
-                out[f"{name}/{kind}_converged"] = np.array([r[4] for r in res], np.int8)
+                full[kind] = {"bits": np.stack([r[0] for r in res]).astype(np.uint8),
+                              "iterations": np.array([r[1] for r in res]),
+                              "ng": np.array([r[2] for r in res], np.uint64),
+                              "ng_p": np.array([r[3] for r in res], np.uint64),
+                              "converged": np.array([r[4] for r in res], np.int8)}
                 print(f"{name} {kind}: {time.time() - t0:.0f}s", flush=True)
-            for kind in ("twin", "crq"):
-                d = np.zeros(n, bool)
-                for f in ("iterations", "ng", "ng_p", "converged"):
-                    d |= out[f"{name}/{kind}_{f}"] != out[f"{name}/ref_{f}"]
-                d |= (out[f"{name}/{kind}_bits"] != out[f"{name}/ref_bits"]).any(axis=1)
-                print(f"{name}: {kind} differs from the reference on {d.sum()} of {n} codewords: "
-                      f"{np.flatnonzero(d).tolist()}", flush=True)
-    # Bits agree between the three decoders except where recorded; store the
-    # reference bits once and the others only where they differ.
-    for name, *_ in SETS:
-        rb = out[f"{name}/ref_bits"]
-        for kind in ("twin", "crq"):
-            kb = out.pop(f"{name}/{kind}_bits")
-            idx = np.flatnonzero((kb != rb).any(axis=1))
-            out[f"{name}/{kind}_bits_diff_idx"] = idx
-            out[f"{name}/{kind}_bits_diff"] = kb[idx]
-    np.savez_compressed(OUT, **out)
-    print(f"wrote {OUT} in {time.time() - t0:.0f}s")
+            # the reference's bits stored once, the others where they differ
+            rb = full["ref"]["bits"]
+            out[f"{name}/ref_bits"] = rb
+            for kind, d in full.items():
+                for f in FIELDS:
+                    out[f"{name}/{kind}_{f}"] = d[f]
+                if kind == "ref":
+                    continue
+                idx = np.flatnonzero((d["bits"] != rb).any(axis=1))
+                out[f"{name}/{kind}_bits_diff_idx"] = idx
+                out[f"{name}/{kind}_bits_diff"] = d["bits"][idx]
+                diff = (d["bits"] != rb).any(axis=1)
+                for f in FIELDS:
+                    diff |= d[f] != full["ref"][f]
+                out[f"{name}/ref_vs_{kind}_idx"] = np.flatnonzero(diff)
+                print(f"{name}: {kind} differs from the glibc-linked reference on {diff.sum()} of {n} "
+                      f"codewords: {np.flatnonzero(diff).tolist()}", flush=True)
+    np.savez_compressed(args.out, **out)
+    print(f"wrote {args.out} in {time.time() - t0:.0f}s")
 
 
 if __name__ == "__main__":

@@ -119,3 +119,18 @@ def test_wait_limit_is_clamped(sg):
         assert lib.sg_set_wait_limit(5) == 0 and lib.sg_get_wait_limit() == 5
     finally:
         lib.sg_set_wait_limit(old)
+
+
+def test_autograd_wrapper_rejects_misshapen_tensors(sg):
+    """The differentiable decode checks dtype, device and layout before it
+    hands pointers to the C ABI (no GPU needed to see the rejection)."""
+    import torch
+
+    from sogrand_b200 import diff
+
+    alpha = torch.full((90,), 0.7, dtype=torch.float64)
+    bits = torch.zeros((2, 4096), dtype=torch.uint8)
+    for bad in (torch.zeros((2, 4096), dtype=torch.float32), torch.zeros((2, 4096), dtype=torch.float64),
+                torch.zeros((4096, 2), dtype=torch.float64).t()):
+        with pytest.raises(ValueError):
+            diff.decode_bce(alpha, bad, bits)

@@ -164,7 +164,10 @@ def test_guess_ceiling_bounds_the_decoder(cuda, sg):
     torch = cuda
     lib = _lib.load()
     ceil = C.c_double()
-    assert lib.sg_guess_ceiling(2000, C.byref(ceil)) == 0
+    assert lib.sg_guess_ceiling(2000, 0, C.byref(ceil)) == 0
+    tab = C.c_double()
+    assert lib.sg_guess_ceiling(2000, 1, C.byref(tab)) == 0 and tab.value > 0
+    assert lib.sg_guess_ceiling(2000, 2, C.byref(tab)) == 1
     _, llr = sg.gen_llr(99, 0, 4096, ebn0_db=2.0, device="cuda")
     sg.decode(llr)
     torch.cuda.synchronize()

@@ -58,6 +58,41 @@ def test_noalloc_matches_regular_entry_twice(cuda, sg, golden):
     assert _summary(out_sum, sg) == expect
 
 
+def test_noalloc_tables_on_high_ic_lines(cuda, sg):
+    """The allocation-free entry point decodes with its own copy of the
+    pattern-order tables, built on the device.  Cubes whose LLR magnitudes
+    are large and of several spreads give lines with reliability shifts (IC)
+    from about 5 to over 100, and 1% flipped signs make those lines search
+    deep into their tables; both entry points must agree, through the
+    summaries, the bits and the total guess count."""
+    torch = cuda
+    lib = _lib.load()
+    rng = np.random.default_rng(31337)
+    code = sg.encode(sg.gen_info(31337, 0, 96)).astype(np.float64)
+    spread = np.repeat([2.0, 6.0, 12.0, 24.0], 24)[:, None]
+    mag = rng.uniform(12.0, 30.0, (96, 1)) + rng.uniform(0.0, 1.0, code.shape) * spread
+    llr = (1.0 - 2.0 * code) * mag
+    flip = rng.random(code.shape) < 0.01
+    llr[flip] = -llr[flip]
+    llr = np.ascontiguousarray(llr)
+    d_llr = torch.from_numpy(llr).cuda()
+    n = llr.shape[0]
+    p = sg.params()
+    want = torch.zeros(sg.SUMMARY_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    want_bits = torch.empty((n, 64), dtype=torch.uint8, device="cuda")
+    assert lib.sg_decode_summary_device(d_llr.data_ptr(), n, C.byref(p), None, want_bits.data_ptr(),
+                                        want.data_ptr(), None) == 0
+    got = torch.zeros(sg.SUMMARY_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    got_bits = torch.empty((n, 64), dtype=torch.uint8, device="cuda")
+    assert lib.sg_decode_summary_device_noalloc(d_llr.data_ptr(), n, C.byref(p), None, got_bits.data_ptr(),
+                                                got.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert _summary(got, sg) == _summary(want, sg)
+    assert torch.equal(got_bits, want_bits)
+    _, st, _ = sg.decode(llr)  # host entry point, regular tables
+    assert _summary(got, sg)["total_ng"] == int(st["ng"].sum())
+
+
 def test_noalloc_rejects_oversize(cuda, sg):
     lib = _lib.load()
     p = sg.params()
