@@ -138,7 +138,11 @@ sg_status sg_bitso_host(const double* llr, size_t n_lines, int32_t L, uint64_t T
  * ignored, as the reference's fread loop does), writes packed bits to
  * out_path (a final partial byte, never produced for 512-bit blocks, would
  * be left-shifted), fills *summary (nullable).  Decodes in chunks of at most
- * chunk_cw codewords (0 = automatic). */
+ * chunk_cw codewords (0 = automatic, at most 8192): a reader thread reads
+ * the next chunk into pinned host memory while earlier chunks are copied
+ * and decoded on the host pipeline's two lanes (the first call on a device
+ * pins 768 MB of staging and keeps it).  Returns SG_ERR_NONFINITE after
+ * decoding the rest if a cube held a non-finite LLR. */
 sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_params* p,
                          size_t chunk_cw, sg_run_summary* summary);
 

@@ -27,9 +27,11 @@
 
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sogrand_b200.h"
@@ -738,6 +740,9 @@ int grid_for(unsigned long long n, int cap)
  * the batch handles below. */
 sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params* p, uint8_t* bits, double* lapp,
                                 sg_cw_stats* stats);
+/* The file decoder's pipeline, defined with them. */
+sg_status decode_file_pipelined(FILE* fi, FILE* fo, const sg_params* p, size_t chunk_cw, sg_run_summary* sum,
+                                bool* any_nonfinite);
 
 } // namespace
 
@@ -882,38 +887,15 @@ sg_status sg_decode_file(const char* in_path, const char* out_path, const sg_par
         fclose(fi);
         return fail(SG_ERR_IO, std::string("Error opening output file: ") + strerror(errno));
     }
-    if (chunk_cw == 0)
-        chunk_cw = 16384;
-    std::vector<double> buf(chunk_cw * SG_CUBE);
-    std::vector<uint8_t> bits(chunk_cw * SG_INFO_BYTES);
-    std::vector<sg_cw_stats> st(chunk_cw);
     sg_run_summary sum;
     memset(&sum, 0, sizeof sum);
-    for (;;) {
-        const size_t got = fread(buf.data(), sizeof(double) * SG_CUBE, chunk_cw, fi);
-        if (got == 0)
-            break;
-        s = sg_decode_host(buf.data(), got, p, bits.data(), nullptr, st.data());
-        if (s != SG_OK)
-            break;
-        if (fwrite(bits.data(), SG_INFO_BYTES, got, fo) != got) {
-            s = fail(SG_ERR_IO, "short write to output file");
-            break;
-        }
-        for (size_t i = 0; i < got; i++) {
-            sum.total_iterations += st[i].iterations;
-            sum.total_ng += st[i].ng;
-            sum.total_ng_p += st[i].ng_p;
-        }
-        sum.blocks += got;
-        if (got < chunk_cw)
-            break;
-    }
-    if (s == SG_OK && ferror(fi))
-        s = fail(SG_ERR_IO, "read error on input file");
+    bool nonfinite = false;
+    s = decode_file_pipelined(fi, fo, p, chunk_cw, &sum, &nonfinite);
     fclose(fi);
     if (fclose(fo) != 0 && s == SG_OK)
         s = fail(SG_ERR_IO, "error closing output file");
+    if (s == SG_OK && nonfinite)
+        s = fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
     sum.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (summary)
         *summary = sum;
@@ -1250,11 +1232,23 @@ struct HostLane {
  * serialised by the mutex. */
 constexpr int SG_HOST_LANES = 2;
 constexpr size_t SG_HOST_CHUNK = 16384;
+/* Pinned host staging of the file decoder: SG_FILE_BUFS chunks of LLR cubes
+ * (a reader thread fills one while the lanes decode the others) and the
+ * bits and statistics of each lane's chunk. */
+constexpr size_t SG_FILE_CHUNK = 8192;
+constexpr int SG_FILE_BUFS = 3;
+struct FileStage {
+    double* llr[SG_FILE_BUFS] = {};
+    uint8_t* bits[SG_HOST_LANES] = {};
+    sg_cw_stats* st[SG_HOST_LANES] = {};
+    bool ready = false;
+};
 struct HostPipe {
     std::mutex mu;
     HostLane ln[SG_HOST_LANES];
     bool ready = false;     /* buffers (without L_APP), streams and queues */
     bool has_lapp = false;  /* L_APP buffers too */
+    FileStage fs;           /* pinned staging, allocated by the first file decode */
 };
 constexpr int SG_HOST_MAX_DEV = 64;
 HostPipe g_host_pipe[SG_HOST_MAX_DEV];
@@ -1367,6 +1361,174 @@ sg_status decode_host_pipelined(const double* llr, size_t n_cw, const sg_params*
         cudaStreamSynchronize(L.st);
     if (s == SG_OK && any_nonfinite)
         return fail(SG_ERR_NONFINITE, "input contains non-finite LLRs; those codewords were not decoded");
+    return s;
+}
+
+sg_status file_stage_setup(FileStage& fs)
+{
+    if (fs.ready)
+        return SG_OK;
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < SG_FILE_BUFS && e == cudaSuccess; b++)
+        e = cudaHostAlloc((void**)&fs.llr[b], SG_FILE_CHUNK * SG_CUBE * sizeof(double), cudaHostAllocDefault);
+    for (int l = 0; l < SG_HOST_LANES && e == cudaSuccess; l++) {
+        e = cudaHostAlloc((void**)&fs.bits[l], SG_FILE_CHUNK * SG_INFO_BYTES, cudaHostAllocDefault);
+        if (e == cudaSuccess)
+            e = cudaHostAlloc((void**)&fs.st[l], SG_FILE_CHUNK * sizeof(sg_cw_stats), cudaHostAllocDefault);
+    }
+    if (e != cudaSuccess) {
+        for (int b = 0; b < SG_FILE_BUFS; b++)
+            cudaFreeHost(fs.llr[b]);
+        for (int l = 0; l < SG_HOST_LANES; l++) {
+            cudaFreeHost(fs.bits[l]);
+            cudaFreeHost(fs.st[l]);
+        }
+        fs = FileStage();
+        return cuda_fail(e, "pinned staging buffers of the file decoder");
+    }
+    fs.ready = true;
+    return SG_OK;
+}
+
+/* The file decoder's pipeline.  A reader thread fills pinned staging
+ * buffers with chunks of whole cubes (fread, as the reference's loop reads
+ * them; a trailing partial cube is ignored); the calling thread copies each
+ * chunk to a lane of the host pipeline, decodes it with the batched decoder
+ * and copies bits and statistics back, alternating between the two lanes,
+ * and writes a chunk's bits when its lane is taken again (chunks are
+ * written in order).  File reading, both copy directions and decoding
+ * overlap.  chunk_cw: codewords per chunk, 0 or above SG_FILE_CHUNK for
+ * SG_FILE_CHUNK. */
+sg_status decode_file_pipelined(FILE* fi, FILE* fo, const sg_params* p, size_t chunk_cw, sg_run_summary* sum,
+                                bool* any_nonfinite)
+{
+    const size_t chunk = (chunk_cw == 0 || chunk_cw > SG_FILE_CHUNK) ? SG_FILE_CHUNK : chunk_cw;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= SG_HOST_MAX_DEV)
+        return fail(SG_ERR_ARG, "device index beyond the host pipeline's table");
+    HostPipe& hp = g_host_pipe[dev];
+    std::lock_guard<std::mutex> lk(hp.mu);
+    sg_status s = host_pipe_setup(hp, dev, false);
+    if (s == SG_OK)
+        s = file_stage_setup(hp.fs);
+    if (s != SG_OK)
+        return s;
+    FileStage& fs = hp.fs;
+
+    /* reader: chunk k goes to buffer k % SG_FILE_BUFS once the chunk that
+     * used it before has been decoded and read back */
+    std::mutex m;
+    std::condition_variable cv;
+    size_t count[SG_FILE_BUFS] = {};
+    bool full[SG_FILE_BUFS] = {};
+    bool stop = false, read_err = false;
+    std::thread reader([&] {
+        for (size_t k = 0;; k++) {
+            const int b = (int)(k % SG_FILE_BUFS);
+            {
+                std::unique_lock<std::mutex> ul(m);
+                cv.wait(ul, [&] { return !full[b] || stop; });
+                if (stop)
+                    return;
+            }
+            const size_t got = fread(fs.llr[b], sizeof(double) * SG_CUBE, chunk, fi);
+            const bool err = got < chunk && ferror(fi);
+            {
+                std::lock_guard<std::mutex> g(m);
+                count[b] = got;
+                full[b] = true;
+                read_err = read_err || err;
+            }
+            cv.notify_all();
+            if (got < chunk)
+                return; /* end of file, or a read error */
+        }
+    });
+
+    HostLane* ln = hp.ln;
+    long pending[SG_HOST_LANES] = {-1, -1}; /* chunk held by each lane */
+    size_t pend_n[SG_HOST_LANES] = {0, 0};
+    auto drain = [&](int l) -> sg_status {
+        if (pending[l] < 0)
+            return SG_OK;
+        HostLane& L = ln[l];
+        SgQueue hq;
+        SG_CUDA(cudaMemcpyAsync(&hq, L.b.q, sizeof hq, cudaMemcpyDeviceToHost, L.st));
+        SG_CUDA(cudaStreamSynchronize(L.st));
+        const size_t n = pend_n[l];
+        {
+            std::lock_guard<std::mutex> g(m);
+            full[pending[l] % SG_FILE_BUFS] = false; /* its input buffer is free again */
+        }
+        cv.notify_all();
+        pending[l] = -1;
+        if (hq.err)
+            return fail(SG_ERR_TIMEOUT, "a persistent-decoder warp gave up waiting for work");
+        if (fwrite(fs.bits[l], SG_INFO_BYTES, n, fo) != n)
+            return fail(SG_ERR_IO, "short write to output file");
+        for (size_t i = 0; i < n; i++) {
+            const sg_cw_stats& c = fs.st[l][i];
+            *any_nonfinite |= c.converged < 0;
+            sum->total_iterations += c.iterations;
+            sum->total_ng += c.ng;
+            sum->total_ng_p += c.ng_p;
+        }
+        sum->blocks += n;
+        return SG_OK;
+    };
+    for (size_t k = 0; s == SG_OK; k++) {
+        const int b = (int)(k % SG_FILE_BUFS), l = (int)(k % SG_HOST_LANES);
+        size_t n;
+        {
+            std::unique_lock<std::mutex> ul(m);
+            cv.wait(ul, [&] { return full[b]; });
+            n = count[b];
+        }
+        if ((s = drain(l)) != SG_OK)
+            break;
+        if (n == 0)
+            break;
+        HostLane& L = ln[l];
+        cudaError_t ce = cudaMemcpyAsync(L.dl, fs.llr[b], n * SG_CUBE * sizeof(double), cudaMemcpyHostToDevice,
+                                         L.st);
+        if (ce != cudaSuccess) {
+            s = cuda_fail(ce, "cudaMemcpyAsync H2D");
+            break;
+        }
+        if ((s = batch_enqueue(&L.b, L.dl, n, p, L.db, nullptr, L.dst, L.st)) != SG_OK)
+            break;
+        if ((ce = cudaMemcpyAsync(fs.bits[l], L.db, n * SG_INFO_BYTES, cudaMemcpyDeviceToHost, L.st)) !=
+                cudaSuccess ||
+            (ce = cudaMemcpyAsync(fs.st[l], L.dst, n * sizeof(sg_cw_stats), cudaMemcpyDeviceToHost, L.st)) !=
+                cudaSuccess) {
+            s = cuda_fail(ce, "cudaMemcpyAsync D2H");
+            break;
+        }
+        pending[l] = (long)k;
+        pend_n[l] = n;
+        if (n < chunk)
+            break; /* the last chunk */
+    }
+    /* the lanes' remaining chunks, in order */
+    const int first = (pending[0] >= 0 && (pending[1] < 0 || pending[0] < pending[1])) ? 0 : 1;
+    for (int i = 0; i < SG_HOST_LANES; i++) {
+        const sg_status d = drain((first + i) % SG_HOST_LANES);
+        if (s == SG_OK)
+            s = d;
+    }
+    {
+        std::lock_guard<std::mutex> g(m);
+        stop = true;
+    }
+    cv.notify_all();
+    reader.join();
+    for (HostLane& L : hp.ln)
+        cudaStreamSynchronize(L.st);
+    if (s == SG_OK && read_err)
+        s = fail(SG_ERR_IO, "read error on input file");
     return s;
 }
 

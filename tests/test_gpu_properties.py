@@ -153,6 +153,38 @@ def test_cli_drop_in(cuda, sg, tmp_path):
     assert out[-1].startswith("Throughput: ")
 
 
+def test_file_decoder_chunks_and_edges(cuda, sg, tmp_path):
+    """sg_decode_file in small chunks (the reader, both lanes and the in-order
+    writes all exercised), with a trailing partial cube (ignored, as the
+    reference's fread loop ignores it) and a non-finite cube (reported after
+    the rest is decoded); and an empty file."""
+    info, llr = sg.gen_llr(8, 0, 40, ebn0_db=2.0)
+    llr = llr.copy()
+    llr[13, 77] = np.nan
+    path = tmp_path / "llr.bin"
+    with open(path, "wb") as f:
+        f.write(llr.tobytes())
+        f.write(b"\0" * 1000)  # partial cube
+    want_bits, want_st, _ = sg.decode(np.delete(llr, 13, axis=0))
+    for chunk in (7, 16, 0):
+        with pytest.raises(sg.SograndError) as ex:
+            sg.decode_file(str(path), str(tmp_path / "dec.bin"), chunk_cw=chunk)
+        assert ex.value.status == 3  # SG_ERR_NONFINITE
+        got = np.frombuffer((tmp_path / "dec.bin").read_bytes(), np.uint8).reshape(-1, 64)
+        assert got.shape[0] == 40 and not got[13].any()
+        assert np.array_equal(np.delete(got, 13, axis=0), want_bits), chunk
+    llr[13, 77] = 0.5
+    path.write_bytes(llr.tobytes())
+    bits, st, _ = sg.decode(llr)
+    s = sg.decode_file(str(path), str(tmp_path / "dec.bin"), chunk_cw=9)
+    assert (tmp_path / "dec.bin").read_bytes() == bits.tobytes()
+    assert s["blocks"] == 40 and s["total_ng"] == int(st["ng"].sum())
+    assert s["total_iterations"] == float(st["iterations"].sum())
+    (tmp_path / "empty.bin").write_bytes(b"")
+    s = sg.decode_file(str(tmp_path / "empty.bin"), str(tmp_path / "dec.bin"))
+    assert s["blocks"] == 0 and (tmp_path / "dec.bin").read_bytes() == b""
+
+
 def test_guess_ceiling_bounds_the_decoder(cuda, sg):
     """The per-guess arithmetic ceiling is positive and above the decoder's
     own guess rate on the same GPU."""
