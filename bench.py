@@ -223,6 +223,74 @@ def cpu_baseline(args):
             "sample": cpu_sample_text(kind, n, per_core, cores) + f"; {dt:.1f} s wall"}
 
 
+_REF_LIB = None
+
+
+def _ref_harness_decode(args):
+    """Pool worker: one codeword through the reference's own functions
+    (oracle/_ref/libsgref.so, glibc libm) at the given Tmax; returns the
+    packed bits."""
+    global _REF_LIB
+    llr, tmax = args
+    if _REF_LIB is None:
+        _REF_LIB = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libsgref.so"))
+        dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+        u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
+        _REF_LIB.sgref_decode.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp, u8,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    bits = np.zeros(64, np.uint8)
+    _REF_LIB.sgref_decode(np.ascontiguousarray(llr), 1, 3, 30, tmax, 1.0 - 1e-5, np.full(100, 0.7), bits, None,
+                          None, None, None, None)
+    return bits
+
+
+def run_sweep(args):
+    """Eb/N0 sweep of the plain method at scale: per point and Tmax, the GPU
+    decode-and-compare of n codewords (codewords/s, BER with 95% interval,
+    iterations, NG; sogrand_b200.sweep) and, beside it, the reference's own
+    decoder on all host cores over the first cores x cpu_cw_per_core
+    codewords of the same stream (one codeword per task from a shared
+    queue), with its decoded bits checked against the GPU's."""
+    import multiprocessing as mp
+
+    import torch
+
+    import sogrand_b200 as sg
+    from sogrand_b200.sweep import parse_points, sweep
+
+    torch.cuda.set_device(0)
+    cores = len(os.sched_getaffinity(0))
+    n_cpu = cores * args.cpu_cw_per_core
+    points = parse_points(args.ebn0)
+    tmaxes = [(1 << 64) - 1 if t == "inf" else int(t) for t in args.tmax.split(",")]
+    have_ref = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsgref.so"))
+    rows = []
+    with mp.get_context("spawn").Pool(cores) as pool:
+        for tmax in tmaxes:
+            p = sg.params(Tmax=tmax)
+            for eb in points:
+                row = sweep([eb], args.n_cw, seed=args.seed, params=p)[0]
+                row["tmax"] = "inf" if tmax == (1 << 64) - 1 else tmax
+                if have_ref and n_cpu > 0:
+                    _, llr = sg.gen_llr(args.seed, 0, n_cpu, ebn0_db=eb)
+                    gbits, _, _ = sg.decode(llr, p)
+                    t0 = time.perf_counter()
+                    rbits = pool.map(_ref_harness_decode, [(llr[i], tmax) for i in range(n_cpu)], chunksize=1)
+                    dt = time.perf_counter() - t0
+                    row["cpu_reference"] = {
+                        "codewords_per_s": n_cpu / dt, "codewords": n_cpu, "cores": cores,
+                        "how": "reference functions (oracle/_ref/libsgref.so, -O2, glibc), one codeword per "
+                               "task from a shared queue over all host cores",
+                        "bits_differing_from_gpu": int(sum(not np.array_equal(a, b) for a, b in zip(rbits, gbits)))}
+                rows.append(row)
+                c = row.get("cpu_reference", {})
+                print(f"Tmax {row['tmax']:>5} {eb:5.2f} dB  GPU {row['codewords_per_s']:9.0f} cw/s  "
+                      f"BER {row['ber']:.3e}  it {row['avg_iterations']:5.2f}  NG {row['ng_per_codeword']:9.0f}  "
+                      f"CPU {c.get('codewords_per_s', 0):7.2f} cw/s ({c.get('bits_differing_from_gpu')})",
+                      flush=True)
+    print(json.dumps({"sweep": rows}), flush=True)
+
+
 def bench_config(args, n, world):
     return {"workload": f"cubic (16,8)^3 SOGRAND decode, {n} codewords per GPU per step, "
                         + (f"Eb/N0 {EBN0} dB" if args.workload == "2dB" else "Eb/N0 U[1,3] dB per codeword")
@@ -250,10 +318,18 @@ def main():
                     help="2dB: Eb/N0 2.0 dB; mixed: per-codeword Eb/N0 uniform in [1, 3] dB")
     ap.add_argument("--variant", default=None, help="decoder kernel variant (name or index)")
     ap.add_argument("--autotune", action="store_true", help="measure all variants first, keep the fastest")
+    ap.add_argument("--sweep", action="store_true",
+                    help="instead of the bench line: Eb/N0 x Tmax sweep with a CPU reference column")
+    ap.add_argument("--ebn0", default="1.0:3.0:0.25", help="sweep points, a:b:step or a comma list (dB)")
+    ap.add_argument("--tmax", default="inf,1000", help="sweep Tmax values, comma list ('inf' = none)")
+    ap.add_argument("--seed", type=int, default=20261203, help="sweep stream seed")
     ap.add_argument("--port-worker", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.port_worker:
         port_worker(args.port_worker)
+        return
+    if args.sweep:
+        run_sweep(args)
         return
     rank, world, local = dist_env()
     if args.impl == "reference":

@@ -243,16 +243,17 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
  * sg_backward_device re-runs every line decode from those checkpoints in
  * reverse phase order and returns, per codeword, the loss
  *   sum_i softplus(s_i L_APP_i),  s_i = +1 for transmitted bit 1, -1 for 0
- * (BCE of the final APP, over all 4096 code bits), its gradient with respect
- * to the per-phase weights alpha (d_grad_alpha[n_cw][3*Imax]) and,
+ * (loss_mode 0: BCE of the final APP, over all 4096 code bits; loss_mode 1:
+ * the same summed over the APP of every phase run), its gradient with
+ * respect to the per-phase weights alpha (d_grad_alpha[n_cw][3*Imax]) and,
  * optionally, to the channel LLRs (d_grad_llr[n_cw][4096]).  Requires
  * Tmax >= 65536.  d_code_bits: [n_cw][4096] bytes 0/1 in cube order. */
 sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
                             double* d_lapp, sg_cw_stats* d_stats, double* d_ckpt, void* stream);
 sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* p,
                              const sg_cw_stats* d_stats, const double* d_ckpt,
-                             const uint8_t* d_code_bits, double* d_loss, double* d_grad_alpha,
-                             double* d_grad_llr, void* stream);
+                             const uint8_t* d_code_bits, int32_t loss_mode, double* d_loss,
+                             double* d_grad_alpha, double* d_grad_llr, void* stream);
 
 /* ---- batched persistent decoder.  One resident CTA per SM holds several
  * codeword slots; warps take lines from any slot with work, the warp that

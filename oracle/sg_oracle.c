@@ -739,8 +739,8 @@ static void line_vjp(const double x[SGO_N], const double g[SGO_N], const line_st
 
 static double softplus(double z) { return z > 0 ? z + log1p(exp(-z)) : log1p(exp(z)); }
 
-void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, double* loss_out,
-                        double* grad_alpha, double* grad_llr)
+void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, int loss_mode,
+                        double* loss_out, double* grad_alpha, double* grad_llr)
 {
     code_init();
     static const int stride[3] = {1, 16, 256};
@@ -799,7 +799,7 @@ void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* c
                     const int q = base + i * stride[axis];
                     gE[i] = gle[q];
                     g[i] = gE[i];
-                    if (ph == P - 1) {
+                    if (ph == P - 1 || loss_mode == 1) { /* the final APP, or every phase's */
                         const double sg = code_bits[q] ? 1.0 : -1.0;
                         const double z = sg * o.lapp[i];
                         loss += softplus(z);

@@ -87,10 +87,11 @@ void sgo_gen_llr(uint64_t seed, uint64_t cw0, size_t n, double sigma, uint8_t* i
 
 /* FP64 adjoint of one codeword's decode (the branch of the forward pass
  * held fixed): loss = sum_i softplus(s_i L_APP_i) over the 4096 code bits,
- * s_i = +1 for bit 1, -1 for 0; grad_alpha[3*Imax] and grad_llr[4096] its
- * gradients.  Requires Tmax = UINT64_MAX. */
-void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, double* loss,
-                        double* grad_alpha, double* grad_llr);
+ * s_i = +1 for bit 1, -1 for 0, of the final APP (loss_mode 0) or summed
+ * over every phase's APP (loss_mode 1); grad_alpha[3*Imax] and
+ * grad_llr[4096] its gradients.  Requires Tmax = UINT64_MAX. */
+void sgo_decode_adjoint(const double* llr, const sgo_params* p, const uint8_t* code_bits, int loss_mode,
+                        double* loss, double* grad_alpha, double* grad_llr);
 double sgo_decode_loss(const double* llr, const sgo_params* p, const uint8_t* code_bits);
 
 /* Which exp/log this build uses: 0 = libm, 1 = sg_math.h. */

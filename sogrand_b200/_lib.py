@@ -106,7 +106,8 @@ _SIGS = {
     "sg_check_device": (C.c_int, [_VP]),
     "sg_guess_ceiling": (C.c_int, [C.c_ulonglong, C.c_int32, C.POINTER(C.c_double)]),
     "sg_forward_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP, _VP]),
-    "sg_backward_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "sg_backward_device": (C.c_int, [_VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, C.c_int32, _VP, _VP, _VP,
+                                     _VP]),
     "sg_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),
     "sg_batch_destroy": (C.c_int, [_VP]),
     "sg_batch_decode": (C.c_int, [_VP, _VP, C.c_size_t, C.POINTER(SgParams), _VP, _VP, _VP, _VP]),

@@ -21,8 +21,9 @@
  * writes one 32 KB checkpoint per phase), accumulating E and E_i on the way,
  * and propagates the gradient of the loss
  *   loss = sum_i softplus(s_i L_APP_i),  s_i = +1 for code bit 1, -1 for 0,
- * (the BCE of the final APP against the transmitted bits) to the per-phase
- * extrinsic weights alpha_p, the channel LLRs and the previous phase.
+ * (the BCE of the final APP against the transmitted bits; loss_mode 1: the
+ * sum of that over every phase's APP) to the per-phase extrinsic weights
+ * alpha_p, the channel LLRs and the previous phase.
  */
 #pragma once
 
@@ -101,6 +102,7 @@ struct SgBackwardArgs {
     unsigned long long n_cw;
     int32_t L;
     int32_t nph;                 /* 3 * Imax */
+    int32_t loss_mode;           /* 0: BCE of the final APP; 1: summed over all phases' APPs */
     double thres;
     double alpha[SG_MAX_PHASES];
 };
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(NW * 32, 3) sg_backward_kernel(const __grid_co
                 const SgLineResult r = sg_decode_line<1, true>(x, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp], &a);
                 const double gE = lane < 16 ? S.gle[pos] : 0.0;
                 double gL = 0.0, lossv = 0.0;
-                if (p == P - 1 && lane < 16) {
+                const bool scored = p == P - 1 || args.loss_mode == 1;
+                if (scored && lane < 16) {
                     const double s = args.code_bits[cw * SG_CUBE + pos] ? 1.0 : -1.0;
                     const double z = s * r.lapp;
                     lossv = z > 0.0 ? z + log1p(exp(-z)) : log1p(exp(z)); /* softplus */
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(NW * 32, 3) sg_backward_kernel(const __grid_co
                 const double ls = sg_sum16(lossv, lane);
                 if (lane == 0) {
                     atomicAdd(&S.ga, ga);
-                    if (p == P - 1)
+                    if (scored)
                         atomicAdd(&S.lsum, ls);
                 }
             }

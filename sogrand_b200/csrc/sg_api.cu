@@ -1714,12 +1714,14 @@ sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p
 }
 
 sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* p, const sg_cw_stats* d_stats,
-                             const double* d_ckpt, const uint8_t* d_code_bits, double* d_loss,
+                             const double* d_ckpt, const uint8_t* d_code_bits, int32_t loss_mode, double* d_loss,
                              double* d_grad_alpha, double* d_grad_llr, void* stream)
 {
     sg_status s = check_params(p);
     if (s != SG_OK)
         return s;
+    if (loss_mode != 0 && loss_mode != 1)
+        return fail(SG_ERR_ARG, "loss_mode must be 0 (final APP) or 1 (every phase's APP)");
     if (p->Tmax < SG_ENUM_LEN && p->Tmax != 0)
         return fail(SG_ERR_ARG, "the adjoint needs Tmax >= 65536 (every line stops at a list insertion)");
     if (n_cw == 0)
@@ -1742,6 +1744,7 @@ sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* 
     a.n_cw = n_cw;
     a.L = p->L;
     a.nph = 3 * p->Imax;
+    a.loss_mode = loss_mode;
     a.thres = p->thres;
     memcpy(a.alpha, p->alpha, sizeof a.alpha);
     void* kargs[] = {(void*)&a};

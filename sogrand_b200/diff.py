@@ -7,6 +7,7 @@ The reference scales the extrinsic information with one constant, alpha =
 3*Imax per-phase weights are trainable: the loss is the BCE of the final
 APP against the transmitted code bits,
     loss = mean over codewords of sum_i softplus(s_i L_APP_i),  s_i = 2 c_i - 1,
+or that BCE summed over the APP of every phase run (loss="phases"),
 differentiated exactly on the branch of the forward pass (sorts, tested
 patterns, lists, stops, early terminations held fixed).  The plain decoder
 with the learned weights is then evaluated by BER.
@@ -50,7 +51,7 @@ def _torch_fn():
 
     class DecodeBCE(torch.autograd.Function):
         @staticmethod
-        def forward(ctx, alpha, llr, code_bits, imax: int, L: int):
+        def forward(ctx, alpha, llr, code_bits, imax: int, L: int, loss_mode: int):
             import sogrand_b200 as sg
 
             lib = _lib.load()
@@ -67,34 +68,30 @@ def _torch_fn():
             s = torch.cuda.current_stream(dev).cuda_stream
             _lib.check(lib.sg_forward_device(llr.data_ptr(), n, C.byref(p), bits.data_ptr(), lapp.data_ptr(),
                                              stats.data_ptr(), ckpt.data_ptr(), s))
-            sgn = code_bits.to(torch.float64) * 2.0 - 1.0
-            loss = torch.nn.functional.softplus(sgn * lapp).sum(dim=1).mean()
-            ctx.save_for_backward(llr, code_bits, ckpt, stats)
-            ctx.p = p
-            ctx.imax = imax
-            ctx.want_llr = llr.requires_grad
-            ctx.bits = bits
-            return loss
+            ctx.imax, ctx.want_llr, ctx.bits = imax, llr.requires_grad, bits
+            if loss_mode == 0:
+                sgn = code_bits.to(torch.float64) * 2.0 - 1.0
+                loss = torch.nn.functional.softplus(sgn * lapp).sum(dim=1).mean()
+                ctx.save_for_backward(llr, code_bits, ckpt, stats)
+                ctx.p, ctx.grads = p, None
+                return loss
+            # every phase's APP: only the backward pass sees the phases, so
+            # it runs now and the gradients are kept for backward()
+            lossv, ga, gl = backward_raw(llr, code_bits, p, stats, ckpt, want_llr=llr.requires_grad, loss_mode=1)
+            ctx.grads = (ga.sum(dim=0) / n, gl / n if gl is not None else None)
+            return lossv.mean()
 
         @staticmethod
         def backward(ctx, g):
-            import sogrand_b200 as sg
-
+            if ctx.grads is not None:
+                ga, gl = ctx.grads
+                return g * ga, (g * gl if gl is not None else None), None, None, None, None
             llr, code_bits, ckpt, stats = ctx.saved_tensors
-            lib = _lib.load()
             n = llr.shape[0]
-            nph = 3 * ctx.imax
-            dev = llr.device
-            loss = torch.empty(n, dtype=torch.float64, device=dev)
-            ga = torch.empty((n, nph), dtype=torch.float64, device=dev)
-            gl = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev) if ctx.want_llr else None
-            s = torch.cuda.current_stream(dev).cuda_stream
-            _lib.check(lib.sg_backward_device(llr.data_ptr(), n, C.byref(ctx.p), stats.data_ptr(),
-                                              ckpt.data_ptr(), code_bits.data_ptr(), loss.data_ptr(),
-                                              ga.data_ptr(), gl.data_ptr() if gl is not None else None, s))
+            _, ga, gl = backward_raw(llr, code_bits, ctx.p, stats, ckpt, want_llr=ctx.want_llr)
             grad_alpha = g * ga.sum(dim=0) / n
             grad_llr = g * gl / n if gl is not None else None
-            return grad_alpha, grad_llr, None, None, None
+            return grad_alpha, grad_llr, None, None, None, None
 
     return DecodeBCE
 
@@ -102,19 +99,23 @@ def _torch_fn():
 _FN = None
 
 
-def decode_bce(alpha, llr, code_bits, imax: int = 30, L: int = 3):
-    """Mean BCE of the final APP over codewords; differentiable in alpha
-    (float64 tensor of 3*imax weights) and in llr (CUDA [n, 4096] float64).
-    code_bits: CUDA uint8 [n, 4096] transmitted bits."""
+def decode_bce(alpha, llr, code_bits, imax: int = 30, L: int = 3, loss: str = "final"):
+    """Mean BCE over codewords, differentiable in alpha (float64 tensor of
+    3*imax weights) and in llr (CUDA [n, 4096] float64).  code_bits: CUDA
+    uint8 [n, 4096] transmitted bits.  loss: "final" -- the BCE of the final
+    APP; "phases" -- the BCE of every phase's APP, summed."""
     global _FN
+    if loss not in ("final", "phases"):
+        raise ValueError("loss must be 'final' or 'phases'")
     if _FN is None:
         _FN = _torch_fn()
     # contiguous() keeps the autograd path to a non-contiguous llr
-    return _FN.apply(alpha, llr.contiguous(), code_bits.contiguous(), imax, L)
+    return _FN.apply(alpha, llr.contiguous(), code_bits.contiguous(), imax, L, 0 if loss == "final" else 1)
 
 
-def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False):
-    """Per-codeword loss and gradients from sg_backward_device (CUDA tensors)."""
+def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False, loss_mode: int = 0):
+    """Per-codeword loss and gradients from sg_backward_device (CUDA tensors);
+    loss_mode 0: BCE of the final APP, 1: summed over every phase's APP."""
     import torch
 
     import sogrand_b200 as sg
@@ -128,7 +129,7 @@ def backward_raw(llr, code_bits, p, stats, ckpt, want_llr: bool = False):
     ga = torch.empty((n, nph), dtype=torch.float64, device=dev)
     gl = torch.empty((n, sg.SG_CUBE), dtype=torch.float64, device=dev) if want_llr else None
     _lib.check(_lib.load().sg_backward_device(llr.data_ptr(), n, C.byref(p), stats.data_ptr(), ckpt.data_ptr(),
-                                              code_bits.data_ptr(), loss.data_ptr(), ga.data_ptr(),
+                                              code_bits.data_ptr(), int(loss_mode), loss.data_ptr(), ga.data_ptr(),
                                               gl.data_ptr() if gl is not None else None,
                                               torch.cuda.current_stream(dev).cuda_stream))
     return loss, ga, gl
@@ -165,7 +166,7 @@ def code_bits_for(info, device):
 
 def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax: int = 30, lr: float = 0.02,
                   seed: int = 90210, device: str = "cuda", init: float = 0.7, log=None, val_cw: int = 0,
-                  val_every: int = 10):
+                  val_every: int = 10, loss: str = "final"):
     """Adam on the 3*imax extrinsic weights over fresh seeded batches (each
     step a new range of the codeword stream).  With val_cw > 0 the mean BCE
     on a fixed validation batch (its own seed) is evaluated every val_every
@@ -186,7 +187,7 @@ def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax
     def validate(step):
         nonlocal best
         with torch.no_grad():
-            v = float(decode_bce(alpha.detach(), vllr, vcb, imax).item())
+            v = float(decode_bce(alpha.detach(), vllr, vcb, imax, loss=loss).item())
         hist["val"].append((step, v))
         if v < best[0]:
             best = (v, alpha.detach().cpu().numpy().copy())
@@ -199,12 +200,12 @@ def train_weights(steps: int = 60, batch: int = 4096, ebn0_db: float = 1.5, imax
         info, llr = sg.gen_llr(seed, step * batch, batch, ebn0_db=ebn0_db, device=device)
         cb = code_bits_for(info, device)
         opt.zero_grad()
-        loss = decode_bce(alpha, llr, cb, imax)
-        loss.backward()
+        lv = decode_bce(alpha, llr, cb, imax, loss=loss)
+        lv.backward()
         opt.step()
         with torch.no_grad():
             alpha.clamp_(0.0, 2.0)
-        hist["train"].append(float(loss.item()))
+        hist["train"].append(float(lv.item()))
         if log:
             log(step, hist["train"][-1], None)
         if val_cw and (step + 1) % val_every == 0:

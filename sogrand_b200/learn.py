@@ -1,16 +1,19 @@
 """Learn per-phase extrinsic weights and evaluate them by BER against the plain
 decoder.
 
-    python -m sogrand_b200.learn --steps 60 --batch 4096 --train-ebn0 1.5 \
+    python -m sogrand_b200.learn --steps 60 --batch 4096 --train-ebn0 1.5 --loss phases \
         --eval-ebn0 1.25,1.5,1.75,2.0 --eval-cw 500000 --eval-imax 5,10,30 --out learned.json
 
 Training: Adam on 3*Imax weights (initialised to the reference's 0.7) with
-the BCE of the final APP on fresh seeded codewords (sogrand_b200.diff).
-Evaluation: the plain decoder (alpha = 0.7, Imax = 30) and the learned
-weights at each Imax decode the same fresh codewords (a codeword range of
-the seeded stream disjoint from training); BER and block error rate come
-with 95% Wilson intervals, and the difference of BERs with a 95% interval
-(normal approximation of the two independent-sample difference).
+the BCE of the final APP, or of every phase's APP (--loss phases), on fresh
+seeded codewords (sogrand_b200.diff).
+Evaluation: the plain decoder (alpha = 0.7, Imax = 30, and at each evaluated
+Imax) and the learned weights at each Imax decode the same fresh codewords
+(a codeword range of the seeded stream disjoint from training).  Every
+decoder sees the same codewords, so BER differences are paired: per
+codeword, d = (bit errors of one decoder) - (bit errors of the other), and
+the 95% interval of the BER difference is mean(d)/512 +- 1.96 sd(d) /
+(512 sqrt(n)).  BER and block error rate come with 95% Wilson intervals.
 """
 from __future__ import annotations
 
@@ -24,44 +27,75 @@ import numpy as np
 Z95 = 1.959963984540054
 
 
-def evaluate(alpha, imax: int, ebn0: float, n_cw: int, seed: int, cw0: int, chunk: int = 100000, variant=None):
+def _popcount_table():
+    import torch
+
+    t = torch.zeros(256, dtype=torch.int16)
+    for i in range(256):
+        t[i] = bin(i).count("1")
+    return t
+
+
+def evaluate_set(configs: dict, ebn0: float, n_cw: int, seed: int, cw0: int, chunk: int = 100000,
+                 pairs=()) -> dict:
+    """Decode the same n_cw fresh codewords with every configuration
+    (name -> (alpha or None for the reference's 0.7, Imax)).  Returns per
+    configuration its totals, and for every (a, b) in pairs the paired BER
+    difference BER(a) - BER(b) with its 95% interval."""
     import torch
 
     import sogrand_b200 as sg
 
-    a = np.full(sg.SG_MAX_PHASES, 0.7)
-    if alpha is not None:
-        a[: min(len(alpha), 3 * imax)] = np.asarray(alpha)[: 3 * imax]
-    p = sg.params(Imax=imax, alpha=a)
-    tot = {k: 0 for k in sg.SUMMARY_DTYPE.names}
-    t = 0.0
+    pop = _popcount_table().cuda()
+    params = {}
+    for name, (alpha, imax) in configs.items():
+        a = np.full(sg.SG_MAX_PHASES, 0.7)
+        if alpha is not None:
+            a[: min(len(alpha), 3 * imax)] = np.asarray(alpha)[: 3 * imax]
+        params[name] = sg.params(Imax=imax, alpha=a)
+    tot = {k: {"bit_errors": 0, "block_errors": 0, "iterations": 0.0, "seconds": 0.0} for k in configs}
+    acc = {pr: [0.0, 0.0] for pr in pairs}  # sum d, sum d^2
     for off in range(0, n_cw, chunk):
         n = min(chunk, n_cw - off)
         info, llr = sg.gen_llr(seed, cw0 + off, n, ebn0_db=ebn0, device="cuda")
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s, _ = sg.decode_summary(llr, p, ref_info=info)
-        t += time.perf_counter() - t0
-        for k in tot:
-            tot[k] += s[k]
+        errs = {}
+        for name, p in params.items():
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            bits, raw, _ = sg.decode(llr, p)
+            e1.record()
+            torch.cuda.synchronize()
+            tot[name]["seconds"] += e0.elapsed_time(e1) / 1000.0
+            e = pop[(bits ^ info).long()].sum(dim=1).to(torch.int64)
+            errs[name] = e
+            tot[name]["bit_errors"] += int(e.sum().item())
+            tot[name]["block_errors"] += int((e > 0).sum().item())
+            tot[name]["iterations"] += float(sg.stats_from_device(raw)["iterations"].sum())
+        for a, b in pairs:
+            d = (errs[a] - errs[b]).to(torch.float64)
+            acc[(a, b)][0] += float(d.sum().item())
+            acc[(a, b)][1] += float((d * d).sum().item())
         del info, llr
-    ber = tot["bit_errors"] / tot["bits_compared"]
-    lo, hi = sg.wilson_interval(tot["bit_errors"], tot["bits_compared"])
-    blo, bhi = sg.wilson_interval(tot["block_errors"], tot["blocks"])
-    return {"imax": imax, "ebn0_db": ebn0, "codewords": tot["blocks"], "bit_errors": tot["bit_errors"],
-            "ber": ber, "ber_ci95": [lo, hi], "block_errors": tot["block_errors"],
-            "bler": tot["block_errors"] / tot["blocks"], "bler_ci95": [blo, bhi],
-            "avg_iterations": tot["total_iterations"] / tot["blocks"], "codewords_per_s": tot["blocks"] / t}
-
-
-def ber_difference(a: dict, b: dict) -> dict:
-    """BER(a) - BER(b) with a 95% normal-approximation interval."""
-    na = a["codewords"] * 512
-    nb = b["codewords"] * 512
-    pa, pb = a["ber"], b["ber"]
-    se = math.sqrt(pa * (1 - pa) / na + pb * (1 - pb) / nb)
-    d = pa - pb
-    return {"diff": d, "ci95": [d - Z95 * se, d + Z95 * se]}
+    out = {"ebn0_db": ebn0, "codewords": n_cw, "configs": {}, "paired": []}
+    for name, t in tot.items():
+        nb = n_cw * 512
+        lo, hi = sg.wilson_interval(t["bit_errors"], nb)
+        blo, bhi = sg.wilson_interval(t["block_errors"], n_cw)
+        out["configs"][name] = {
+            "imax": configs[name][1], "learned": configs[name][0] is not None, "bit_errors": t["bit_errors"],
+            "ber": t["bit_errors"] / nb, "ber_ci95": [lo, hi], "block_errors": t["block_errors"],
+            "bler": t["block_errors"] / n_cw, "bler_ci95": [blo, bhi],
+            "avg_iterations": t["iterations"] / n_cw, "codewords_per_s": n_cw / t["seconds"]}
+    for (a, b), (s1, s2) in acc.items():
+        mean = s1 / n_cw
+        var = max(s2 / n_cw - mean * mean, 0.0) * n_cw / max(n_cw - 1, 1)
+        se = math.sqrt(var / n_cw)
+        d = mean / 512
+        out["paired"].append({"a": a, "b": b, "ber_diff": d,
+                              "ci95": [d - Z95 * se / 512, d + Z95 * se / 512],
+                              "rel": d / out["configs"][b]["ber"] if out["configs"][b]["ber"] else None})
+    return out
 
 
 def main():
@@ -71,6 +105,7 @@ def main():
     ap.add_argument("--train-ebn0", type=float, default=1.5)
     ap.add_argument("--imax-train", type=int, default=30)
     ap.add_argument("--lr", type=float, default=0.02)
+    ap.add_argument("--loss", default="final", choices=["final", "phases"])
     ap.add_argument("--weights", default=None, help="json with learned weights (skip training)")
     ap.add_argument("--val-cw", type=int, default=0, help="validation codewords (keep the best weights)")
     ap.add_argument("--val-every", type=int, default=10)
@@ -90,25 +125,26 @@ def main():
     else:
         alpha, hist = diff.train_weights(steps=args.steps, batch=args.batch, ebn0_db=args.train_ebn0,
                                          imax=args.imax_train, lr=args.lr, seed=args.seed, val_cw=args.val_cw,
-                                         val_every=args.val_every,
+                                         val_every=args.val_every, loss=args.loss,
                                          log=lambda s, l, v: print(f"step {s} loss {l:.4f} val {v}", flush=True))
     train_s = time.perf_counter() - t0
-    res = {"weights": [float(x) for x in alpha], "train": {"steps": args.steps, "batch": args.batch,
-                                                          "val_cw": args.val_cw,
-                                                          "ebn0_db": args.train_ebn0, "imax": args.imax_train,
-                                                          "lr": args.lr, "loss": hist, "seconds": train_s},
+    res = {"weights": [float(x) for x in alpha],
+           "train": {"steps": args.steps, "batch": args.batch, "val_cw": args.val_cw, "loss": args.loss,
+                     "ebn0_db": args.train_ebn0, "imax": args.imax_train, "lr": args.lr, "history": hist,
+                     "seconds": train_s},
            "eval": []}
     eval_seed = args.seed + 1  # a stream disjoint from training
+    imaxes = [int(x) for x in args.eval_imax.split(",")]
+    configs = {"plain30": (None, 30)}
+    pairs = []
+    for im in imaxes:
+        configs[f"learned{im}"] = (alpha, im)
+        pairs.append((f"learned{im}", "plain30"))
+        if im != 30:
+            configs[f"plain{im}"] = (None, im)
+            pairs.append((f"learned{im}", f"plain{im}"))
     for eb in [float(x) for x in args.eval_ebn0.split(",")]:
-        plain = evaluate(None, 30, eb, args.eval_cw, eval_seed, 0)
-        row = {"ebn0_db": eb, "plain_imax30": plain, "learned": [], "plain": []}
-        for im in [int(x) for x in args.eval_imax.split(",")]:
-            r = evaluate(alpha, im, eb, args.eval_cw, eval_seed, 0)
-            r["ber_minus_plain_imax30"] = ber_difference(r, plain)
-            pl = plain if im == 30 else evaluate(None, im, eb, args.eval_cw, eval_seed, 0)
-            r["ber_minus_plain_same_imax"] = ber_difference(r, pl)
-            row["learned"].append(r)
-            row["plain"].append(pl)
+        row = evaluate_set(configs, eb, args.eval_cw, eval_seed, 0, pairs=pairs)
         res["eval"].append(row)
         print(json.dumps(row), flush=True)
     if args.out:

@@ -81,17 +81,17 @@ def twin_decode_one(args):
     return bits[0], stats[0], lapp[0]
 
 
-def adjoint(lib_path, llr, code_bits, **kw):
+def adjoint(lib_path, llr, code_bits, loss_mode=0, **kw):
     """C FP64 adjoint of one codeword: (loss, grad_alpha[3*Imax], grad_llr[4096])."""
     o = Oracle(lib_path)
     lib = o.lib
-    lib.sgo_decode_adjoint.argtypes = [_DP, C.POINTER(OParams), _U8, C.POINTER(C.c_double), _DP, _DP]
+    lib.sgo_decode_adjoint.argtypes = [_DP, C.POINTER(OParams), _U8, C.c_int, C.POINTER(C.c_double), _DP, _DP]
     p = o.params(**kw)
     ga = np.zeros(3 * p.Imax)
     gl = np.zeros(4096)
     loss = C.c_double()
     lib.sgo_decode_adjoint(np.ascontiguousarray(llr, dtype=np.float64), C.byref(p),
-                           np.ascontiguousarray(code_bits, dtype=np.uint8), C.byref(loss), ga, gl)
+                           np.ascontiguousarray(code_bits, dtype=np.uint8), int(loss_mode), C.byref(loss), ga, gl)
     return loss.value, ga, gl
 
 

@@ -11,12 +11,14 @@ pytestmark = pytest.mark.gpu
 
 
 def _c_adjoint(args):
-    path, llr, bits, imax = args
-    return adjoint(path, llr, bits, Imax=imax)
+    path, llr, bits, imax, mode = args
+    return adjoint(path, llr, bits, loss_mode=mode, Imax=imax)
 
 
-@pytest.mark.parametrize("imax", [3, 30])
-def test_gpu_adjoint_matches_c_adjoint(cuda, sg, oracle_paths, imax):
+@pytest.mark.parametrize("imax,mode", [(3, 0), (30, 0), (3, 1), (30, 1)])
+def test_gpu_adjoint_matches_c_adjoint(cuda, sg, oracle_paths, imax, mode):
+    """Loss and gradients of the final APP's BCE (mode 0) and of the BCE
+    summed over every phase's APP (mode 1)."""
     torch = cuda
     from sogrand_b200 import diff
 
@@ -26,10 +28,10 @@ def test_gpu_adjoint_matches_c_adjoint(cuda, sg, oracle_paths, imax):
     d = torch.from_numpy(llr).cuda()
     db = torch.from_numpy(bits).cuda()
     _, stats, lapp, ckpt = diff.forward_raw(d, p)
-    loss, ga, gl = diff.backward_raw(d, db, p, stats, ckpt, want_llr=True)
+    loss, ga, gl = diff.backward_raw(d, db, p, stats, ckpt, want_llr=True, loss_mode=mode)
     torch.cuda.synchronize()
     with mp.get_context("spawn").Pool(4) as pool:
-        ref = pool.map(_c_adjoint, [(oracle_paths["twin"], llr[i], bits[i], imax) for i in range(4)])
+        ref = pool.map(_c_adjoint, [(oracle_paths["twin"], llr[i], bits[i], imax, mode) for i in range(4)])
     for i, (cl, cga, cgl) in enumerate(ref):
         assert abs(loss[i].item() - cl) <= 1e-12 * abs(cl)
         g = ga[i].cpu().numpy()
