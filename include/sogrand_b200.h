@@ -247,7 +247,8 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
  * the same summed over the APP of every phase run), its gradient with
  * respect to the per-phase weights alpha (d_grad_alpha[n_cw][3*Imax]) and,
  * optionally, to the channel LLRs (d_grad_llr[n_cw][4096]).  Requires
- * Tmax >= 65536.  d_code_bits: [n_cw][4096] bytes 0/1 in cube order. */
+ * Tmax >= 65536.  d_code_bits: [n_cw][4096] bytes 0/1 in cube order.
+ * Both use the table-driven exp/log (math mode 0) whatever the mode set. */
 sg_status sg_forward_device(const double* d_llr, size_t n_cw, const sg_params* p, uint8_t* d_bits,
                             double* d_lapp, sg_cw_stats* d_stats, double* d_ckpt, void* stream);
 sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* p,
@@ -281,6 +282,23 @@ int sg_batch_variant_count(void);
 const char* sg_batch_variant_name(int v);
 sg_status sg_batch_set_variant(int v);
 int sg_batch_get_variant(void);
+
+/* ---- math mode (process-wide; launches after the call).  The reference's
+ * guess counts depend on the last bits of its libm's exp and log.
+ *   0 (default): the decoder's table-driven exp/log (within 0.51 ulp; Tang's
+ *     method): fastest; every result equals the oracle restatement built
+ *     with the same routines, and the glibc-linked reference on all but a
+ *     few tenths of a percent of codewords (where glibc's own misrounding
+ *     moves a discrete decision);
+ *   1: correctly rounded exp/log: every result -- bits, statistics and soft
+ *     values -- equals the unmodified reference compiled against any
+ *     correctly rounded libm; about 1.6x the decode time.
+ * Applies to sg_decode_device, sg_decode_host, sg_decode_file,
+ * sg_decode_summary_device(_noalloc), sg_batch_* and sg_bitso_*; the
+ * differentiable pair sg_forward_device / sg_backward_device always uses
+ * mode 0. */
+sg_status sg_set_math_mode(int32_t mode);
+int32_t sg_get_math_mode(void);
 
 /* ---- kernel configuration (process-wide).  Variants differ in warps per
  * codeword CTA and in where the 32 KB channel cube is held (shared memory,
@@ -316,10 +334,10 @@ sg_status sg_check_device(void* stream);
 /* Measured ceiling of the per-guess floating-point work on the current
  * device: one path-metric addition, one exp(-PM) and one P_notGuess
  * subtraction per guess, all SMs, no memory traffic; 2*iters guesses per
- * thread.  mode 0: with the decoder's correctly rounded exp; mode 1: with
- * the table-driven exp of the generator (within 0.51 ulp).  Synchronous.
- * The decoder's guesses/s divided by the mode-0 figure is its fraction of
- * the arithmetic bound. */
+ * thread.  mode 0: with the table-driven exp (math mode 0); mode 1: with the
+ * correctly rounded exp (math mode 1).  Synchronous.  The decoder's
+ * guesses/s divided by the figure of its math mode is its fraction of the
+ * arithmetic bound. */
 sg_status sg_guess_ceiling(unsigned long long iters, int32_t mode, double* guesses_per_second);
 
 /* The order in which a line decode tests error patterns when its

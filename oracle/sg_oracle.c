@@ -8,8 +8,9 @@
  *   C = SOGRAND_C/channel_sim.c
  *
  * Compile with -DSGO_TWIN=1 to evaluate exp/log with the kernel's own
- * routines (sogrand_b200/csrc/sg_crmath.h) instead of libm, and with
- * -DSGO_CRQ=1 with the binary128-based correctly rounded ones of crq.h.
+ * routines instead of libm (-DSG_CR_MATH=1: its correctly rounded ones,
+ * sogrand_b200/csrc/sg_crmath.h), and with -DSGO_CRQ=1 with the
+ * binary128-based correctly rounded ones of crq.h.
  */
 #include "sg_oracle.h"
 
@@ -33,14 +34,14 @@ static double ox_exp(double x) { return crq_exp(x); }
 static double ox_log(double x) { return crq_log(x); }
 static double ox_pow2_neg(double s) { return pow(2.0, -s); }
 #elif SGO_TWIN
-/* the decoder's own exp/log: correctly rounded (sg_crmath.h), or, built
- * with SG_CR_MATH=0, the table-driven routines of sg_math.h -- as the
- * kernel is built */
+/* the decoder's own exp/log: the table-driven routines of sg_math.h (its
+ * default math mode), or, built with SG_CR_MATH=1, the correctly rounded
+ * ones of sg_crmath.h (its reference-exact mode) */
 #include "../sogrand_b200/csrc/sg_crmath.h"
 static const double k_etab[SG_EXP_TAB_LEN] = SG_EXP_TAB_INIT;
 static const double k_ltab[SG_LOG_TAB_LEN] = SG_LOG_TAB_INIT;
 #ifndef SG_CR_MATH
-#define SG_CR_MATH 1
+#define SG_CR_MATH 0
 #endif
 #if SG_CR_MATH
 static double ox_exp(double x) { return sg_exp_cr(x, k_etab); }

@@ -24,7 +24,7 @@ from ._lib import (SG_CUBE, SG_INFO_BYTES, SG_MAX_PHASES, SgCwStats, SgParams,
 __all__ = [
     "SG_CUBE", "SG_INFO_BYTES", "STATS_DTYPE", "SograndError", "params", "reference_alpha",
     "decode", "bitso", "decode_file", "decode_summary", "wilson_interval", "SUMMARY_DTYPE", "channel_sigma", "gen_info", "encode", "gen_llr",
-    "set_wait_limit", "get_wait_limit", "check_device", "version",
+    "set_math_mode", "get_math_mode", "set_wait_limit", "get_wait_limit", "check_device", "version",
 ]
 
 UINT64_MAX = (1 << 64) - 1
@@ -174,6 +174,17 @@ def check_device(stream=None) -> None:
     bounded wait of a plain-decoder kernel gave up on the current device
     since the last check (the flag is cleared)."""
     check(_lib.load().sg_check_device(stream))
+
+
+def set_math_mode(mode: int) -> None:
+    """0: table-driven exp/log (default, fastest); 1: correctly rounded
+    exp/log, bit-exact with the reference under a correctly rounded libm.
+    Process-wide, for launches made after the call."""
+    check(_lib.load().sg_set_math_mode(int(mode)))
+
+
+def get_math_mode() -> int:
+    return int(_lib.load().sg_get_math_mode())
 
 
 def wilson_interval(k: int, n: int, conf_z: float = 1.959963984540054) -> tuple[float, float]:

@@ -101,6 +101,8 @@ _SIGS = {
         [C.c_uint64, C.c_uint64, C.c_size_t, C.c_double, C.c_double, C.c_double, _VP, _VP, _VP],
     ),
     "sg_pattern_order": (C.c_size_t, [C.c_int32, _VP, C.c_size_t]),
+    "sg_set_math_mode": (C.c_int, [C.c_int32]),
+    "sg_get_math_mode": (C.c_int32, []),
     "sg_set_wait_limit": (C.c_int, [C.c_uint64]),
     "sg_get_wait_limit": (C.c_uint64, []),
     "sg_check_device": (C.c_int, [_VP]),

@@ -46,7 +46,7 @@ __device__ __forceinline__ double sg_line_vjp(double x, double g, const SgAdjOut
     const double eps = 1e-40;
     const bool pnl_live = a.pnl > eps;
     const double p_nl = fmax(a.pnl, eps);
-    const double ex = SG_EXP(act ? x : 0.0, etab);
+    const double ex = sg_exp(act ? x : 0.0, etab);
     const double pp1r = 1.0 / (1.0 + ex);
     const double pp0r = 1.0 - pp1r;
     const double pp1 = fmin(fmax(pp1r, eps), 1.0);
@@ -72,7 +72,7 @@ __device__ __forceinline__ double sg_line_vjp(double x, double g, const SgAdjOut
         gx -= a1 * p_nl * dsig;
     const double ax = fabs(x);
     const double sgn = x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0);
-    const double sm = ax <= 50.0 ? 1.0 / (1.0 + SG_EXP(ax, etab)) : 0.0; /* sigma(-|x|) */
+    const double sm = ax <= 50.0 ? 1.0 / (1.0 + sg_exp(ax, etab)) : 0.0; /* sigma(-|x|) */
     for (int j = 0; j < a.curl; j++) {
         const double pj = __shfl_sync(SG_FULL, a.my_e, j);
         const uint32_t cm = __shfl_sync(SG_FULL, a.my_cm, j);

@@ -179,7 +179,7 @@ __device__ __forceinline__ uint32_t sg_smem_u32(const void* p)
 
 extern __shared__ __align__(128) unsigned char sg_smem_raw[];
 
-template <int NW, bool LCH_SMEM, int MINB, int G>
+template <int NW, bool LCH_SMEM, int MINB, int G, bool CR>
 __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
 {
     constexpr int NT = NW * 32;
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
                             args.ckpt[(cw * (3ull * args.imax) + 3 * (iter - 1) + axis) * SG_CUBE + pos] = S.le[pos];
                     }
                     const SgLineResult r =
-                        sg_decode_line<G>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+                        sg_decode_line<G, false, CR>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
                     if (lane < 16) {
                         S.le[pos] = r.le;
                         if (args.lapp)
@@ -353,6 +353,7 @@ struct SgLineSmem {
     SgWarpScratch ws[SG_WARPS];
 };
 
+template <bool CR>
 __global__ void __launch_bounds__(SG_THREADS) sg_bitso_kernel(const double* __restrict__ llr,
                                                                unsigned long long n_lines,
                                                                SgLineParams lp, double* lapp, double* le,
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(SG_THREADS) sg_bitso_kernel(const double* __re
             }
             continue;
         }
-        const SgLineResult r = sg_decode_line<1>(v, lp, enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+        const SgLineResult r = sg_decode_line<1, false, CR>(v, lp, enum_tabs, S.etab, S.ltab, &S.ws[warp]);
         if (lane < 16) {
             lapp[l * 16 + lane] = r.lapp;
             le[l * 16 + lane] = r.le;
@@ -506,11 +507,13 @@ struct SgVariant {
     int nw;
     bool lch_smem;
     size_t smem;
-    const void* fn;
+    const void* fn;    /* table-driven exp/log */
+    const void* fn_cr; /* correctly rounded exp/log (the reference-exact mode) */
 };
 
-#define SG_VARIANT(NW, L, M, G, NAME) \
-    { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M, G> }
+#define SG_VARIANT(NW, L, M, G, NAME)                                                               \
+    { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M, G, false>, \
+      (const void*)sg_decode_kernel<NW, L, M, G, true> }
 static const SgVariant g_variants[] = {
     SG_VARIANT(8, false, 3, 1, "w8-gmem"),
     SG_VARIANT(8, true, 2, 1, "w8-smem"),
@@ -529,10 +532,12 @@ struct SgPVariant {
     int nw;
     int slots;
     size_t smem;
-    const void* fn;
+    const void* fn;    /* table-driven exp/log */
+    const void* fn_cr; /* correctly rounded exp/log (the reference-exact mode) */
 };
-#define SG_PVARIANT(NW, C, G, NAME) \
-    { NAME, NW, C, sizeof(SgPersistSmem<NW, C>), (const void*)sg_persist_kernel<NW, C, G> }
+#define SG_PVARIANT(NW, C, G, NAME)                                                                \
+    { NAME, NW, C, sizeof(SgPersistSmem<NW, C>), (const void*)sg_persist_kernel<NW, C, G, false>, \
+      (const void*)sg_persist_kernel<NW, C, G, true> }
 static const SgPVariant g_pvariants[] = {
     SG_PVARIANT(24, 3, 1, "p24x3"),
     SG_PVARIANT(28, 3, 1, "p28x3"),
@@ -649,6 +654,7 @@ struct DevCtx {
 
 std::mutex g_mu;
 std::atomic<long long> g_wait_limit{SG_WAIT_LIMIT_DEFAULT};
+std::atomic<int> g_math_mode{0}; /* 0: table-driven exp/log, 1: correctly rounded */
 int g_pvariant = 5; /* p32x3-g2: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
 int g_variant = 4; /* w16-gmem-g2: fastest on B200 at 2 dB (sogrand_b200.autotune) */
 DevCtx g_ctx[64];
@@ -693,12 +699,18 @@ sg_status get_ctx(DevCtx** out)
         SG_CUDA(cudaMemcpyToSymbol(c_hcol, g_code.hcol, sizeof g_code.hcol));
         SG_CUDA(cudaMemcpyToSymbol(c_prow, g_code.prow, sizeof g_code.prow));
         SG_CUDA(cudaMemcpyToSymbol(c_ptab, g_code.ptab, sizeof g_code.ptab));
-        for (int v = 0; v < SG_NVARIANTS; v++)
+        for (int v = 0; v < SG_NVARIANTS; v++) {
             SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)g_variants[v].smem));
-        for (int v = 0; v < SG_NPVARIANTS; v++)
+            SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn_cr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_variants[v].smem));
+        }
+        for (int v = 0; v < SG_NPVARIANTS; v++) {
             SG_CUDA(cudaFuncSetAttribute(g_pvariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)g_pvariants[v].smem));
+            SG_CUDA(cudaFuncSetAttribute(g_pvariants[v].fn_cr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_pvariants[v].smem));
+        }
         SG_CUDA(cudaFuncSetAttribute(sg_backward_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(SgBackSmem<8>)));
         SG_CUDA(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
@@ -795,7 +807,8 @@ sg_status sg_decode_device(const double* d_llr, size_t n_cw, const sg_params* p,
     const SgVariant& v = g_variants[g_variant];
     const int grid = grid_for(n_cw, 1 << 30);
     void* kargs[] = {(void*)&a};
-    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem, (cudaStream_t)stream));
+    SG_CUDA(cudaLaunchKernel(g_math_mode.load() ? v.fn_cr : v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem,
+                             (cudaStream_t)stream));
     return SG_OK;
 }
 
@@ -817,8 +830,12 @@ sg_status sg_bitso_device(const double* d_llr, size_t n_lines, int32_t L, uint64
     lp.tmax = tmax_eff(Tmax);
     lp.thres = thres;
     const unsigned long long blocks = (n_lines + SG_WARPS - 1) / SG_WARPS;
-    sg_bitso_kernel<<<grid_for(blocks, 148 * 64), SG_THREADS, 0, (cudaStream_t)stream>>>(
-        d_llr, n_lines, lp, d_lapp, d_le, d_nguess, d_ncw, c->enum_tabs);
+    if (g_math_mode.load())
+        sg_bitso_kernel<true><<<grid_for(blocks, 148 * 64), SG_THREADS, 0, (cudaStream_t)stream>>>(
+            d_llr, n_lines, lp, d_lapp, d_le, d_nguess, d_ncw, c->enum_tabs);
+    else
+        sg_bitso_kernel<false><<<grid_for(blocks, 148 * 64), SG_THREADS, 0, (cudaStream_t)stream>>>(
+            d_llr, n_lines, lp, d_lapp, d_le, d_nguess, d_ncw, c->enum_tabs);
     SG_CUDA(cudaGetLastError());
     return SG_OK;
 }
@@ -1080,9 +1097,12 @@ sg_status noalloc_setup(NoAllocCtx** out)
         SG_CUDA(cudaMemcpyToSymbol(c_hcol, code.hcol, sizeof code.hcol));
         SG_CUDA(cudaMemcpyToSymbol(c_prow, code.prow, sizeof code.prow));
         SG_CUDA(cudaMemcpyToSymbol(c_ptab, code.ptab, sizeof code.ptab));
-        for (int v = 0; v < SG_NVARIANTS; v++)
+        for (int v = 0; v < SG_NVARIANTS; v++) {
             SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)g_variants[v].smem));
+            SG_CUDA(cudaFuncSetAttribute(g_variants[v].fn_cr, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g_variants[v].smem));
+        }
         /* the completion flags of the build borrow the scratch array */
         unsigned int* ok = reinterpret_cast<unsigned int*>(c.scratch);
         SG_CUDA(cudaMemset(ok, 0, SG_ENUM_NTAB * sizeof(unsigned int)));
@@ -1151,7 +1171,8 @@ sg_status sg_decode_summary_device_noalloc(const double* d_llr, size_t n_cw, con
     memcpy(a.alpha, p->alpha, sizeof a.alpha);
     const SgVariant& v = g_variants[g_variant];
     void* kargs[] = {(void*)&a};
-    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid_for(n_cw, 1 << 30)), dim3(v.nw * 32), kargs, v.smem, st));
+    SG_CUDA(cudaLaunchKernel(g_math_mode.load() ? v.fn_cr : v.fn, dim3(grid_for(n_cw, 1 << 30)),
+                             dim3(v.nw * 32), kargs, v.smem, st));
     sg_summary_kernel<<<grid_for((n_cw + 255) / 256, 148 * 8), 256, 0, st>>>(stats, bits, d_ref_info, n_cw, err,
                                                                               d_summary);
     SG_CUDA(cudaGetLastError());
@@ -1210,7 +1231,8 @@ sg_status batch_enqueue(sg_batch b, const double* d_llr, size_t n_cw, const sg_p
     SgQueue* q = b->q;
     void* kargs[] = {(void*)&a, (void*)&q};
     const int grid = (int)(n_cw < (size_t)c->sms ? n_cw : (size_t)c->sms);
-    SG_CUDA(cudaLaunchKernel(v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem, st));
+    SG_CUDA(cudaLaunchKernel(g_math_mode.load() ? v.fn_cr : v.fn, dim3(grid), dim3(v.nw * 32), kargs, v.smem,
+                             st));
     return SG_OK;
 }
 
@@ -1651,7 +1673,7 @@ sg_status sg_guess_ceiling(unsigned long long iters, int32_t mode, double* guess
     if (!guesses_per_second || iters == 0 || (mode != 0 && mode != 1))
         return fail(SG_ERR_ARG, "need iters > 0, mode 0 or 1 and an output pointer");
     void (*kern)(unsigned long long, double*) =
-        mode == 0 ? sg_guess_ceiling_kernel<true> : sg_guess_ceiling_kernel<false>;
+        mode == 1 ? sg_guess_ceiling_kernel<true> : sg_guess_ceiling_kernel<false>;
     DevCtx* c = nullptr;
     sg_status s = get_ctx(&c);
     if (s != SG_OK)
@@ -1752,6 +1774,16 @@ sg_status sg_backward_device(const double* d_llr, size_t n_cw, const sg_params* 
                              sizeof(SgBackSmem<8>), (cudaStream_t)stream));
     return SG_OK;
 }
+
+sg_status sg_set_math_mode(int32_t mode)
+{
+    if (mode != 0 && mode != 1)
+        return fail(SG_ERR_ARG, "math mode must be 0 (table-driven) or 1 (correctly rounded)");
+    g_math_mode.store(mode);
+    return SG_OK;
+}
+
+int32_t sg_get_math_mode(void) { return g_math_mode.load(); }
 
 sg_status sg_set_wait_limit(uint64_t limit)
 {

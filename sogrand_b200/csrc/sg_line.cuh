@@ -44,33 +44,27 @@
 #include "sg_enum.h"
 #include "sg_math.h"
 
-/* The decoder's exp and log.  SG_CR_MATH = 1 (default): correctly rounded
- * (sg_crmath.h), so that results equal the reference's under any correctly
- * rounded libm; 0: the table-driven routines of sg_math.h (within 0.51 ulp),
- * kept for comparison. */
-#ifndef SG_CR_MATH
-#define SG_CR_MATH 1
-#endif
-/* SG_EXP_HYBRID (with SG_CR_MATH): the guess loop first evaluates the
- * table-driven exp (within 0.51 ulp, so the correctly rounded value is the
- * same double or a neighbour) and keeps it wherever that cannot change the
- * result -- a step that P_notGuess crosses by the exact integer sum, where
- * only round(e / ulp(P)) enters and every term is at least 2^-51 of its own
- * magnitude away from a rounding tie; every other step (codewords, binade
- * crossings, near-ties) re-evaluates the correctly rounded exp of all its
- * patterns and uses those throughout. */
-#ifndef SG_EXP_HYBRID
-#define SG_EXP_HYBRID SG_CR_MATH
-#endif
-#if SG_CR_MATH
-#define SG_EXP(x, t) sg_exp_cr(x, t)
-#define SG_EXP_NEG(x, t) sg_exp_cr_neg(x, t)
-#define SG_LOG(x, t) sg_log_cr(x, t)
-#else
-#define SG_EXP(x, t) sg_exp(x, t)
-#define SG_EXP_NEG(x, t) sg_exp_neg(x, t)
-#define SG_LOG(x, t) sg_log(x, t)
-#endif
+/* The decoder's exp and log, chosen per instantiation by the template
+ * parameter CR of sg_decode_line: false (the default decoder) -- the
+ * table-driven routines of sg_math.h, within 0.51 ulp; true (the
+ * reference-exact mode) -- the correctly rounded routines of sg_crmath.h,
+ * with which every result equals the reference's under a correctly rounded
+ * libm, at about 2x the cost per exp. */
+template <bool CR>
+__device__ __forceinline__ double sg_dec_exp(double x, const double* tab)
+{
+    return CR ? sg_exp_cr(x, tab) : sg_exp(x, tab);
+}
+template <bool CR>
+__device__ __forceinline__ double sg_dec_exp_neg(double x, const double* tab)
+{
+    return CR ? sg_exp_cr_neg(x, tab) : sg_exp_neg(x, tab);
+}
+template <bool CR>
+__device__ __forceinline__ double sg_dec_log(double x, const double* tab)
+{
+    return CR ? sg_log_cr(x, tab) : sg_log(x, tab);
+}
 
 #define SG_FULL 0xffffffffu
 
@@ -283,7 +277,7 @@ struct SgAdjOut {
 /* Decode one line.  llr: this lane's input LLR (lanes 0..15; others
  * ignored).  enum_tabs: SG_ENUM_NTAB tables of SG_ENUM_LEN entries.
  * etab/ltab: shared-memory copies of the exp/log tables. */
-template <int G, bool ADJ = false>
+template <int G, bool ADJ = false, bool CR = false>
 __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineParams& lp,
                                                         const uint32_t* __restrict__ enum_tabs,
                                                         const double* etab, const double* ltab,
@@ -301,10 +295,10 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
      * for the sorted PM increments below */
     const double a_all = __shfl_sync(SG_FULL, a, lane & 15);
     const double xj = act ? -a_all : a_all;
-    const double ex = SG_EXP(xj, etab);
+    const double ex = sg_dec_exp<CR>(xj, etab);
     /* JacLog(xj) = xj if xj > 50, 0 if xj < -50, else log(1 + e^xj) (:762),
      * with its exp kept */
-    const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : SG_LOG(1.0 + ex, ltab));
+    const double jl = xj > 50 ? xj : (xj < -50 ? 0.0 : sg_dec_log<CR>(1.0 + ex, ltab));
     const double jn = act ? jl : 0.0;
     {
         /* the soft output's exp(LLR) of position p is this exp of lane p + 16
@@ -487,9 +481,8 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
             break;
         }
         /* G patterns per lane: lane j of half h tests pattern base + 32h + j */
-        constexpr bool HYB = SG_EXP_HYBRID && !ADJ;
         uint32_t ent[G];
-        double e[G], pmv[G];
+        double e[G];
         uint32_t hits[G];
         int nv[G];
         int nvt = 0; /* valid patterns of the step, in order */
@@ -542,8 +535,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                     rest &= rest - 1u;
                 }
             }
-            pmv[h] = pm;
-            e[h] = HYB ? sg_exp_neg(-pm, etab) : SG_EXP_NEG(-pm, etab);
+            e[h] = sg_dec_exp_neg<CR>(-pm, etab);
             hits[h] = __ballot_sync(SG_FULL, syn == 0u) & (nv[h] >= 32 ? SG_FULL : ((1u << nv[h]) - 1u));
             nvt += nv[h];
         }
@@ -568,11 +560,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
                 const double q = lane < nv[h] ? __dmul_rn(e[h], iu) : 0.0;
                 const double t = __dadd_rn(q, 0x1p52);
                 const double d = __dsub_rn(t, 0x1p52);
-                /* a tie (or, with the table-driven exp, anything within
-                 * q 2^-51 >= 2 ulp(q) of one) goes to the general case */
-                bad |= !(q < 0x1p52) ||
-                       (HYB ? fabs(__dsub_rn(q, d)) >= __dsub_rn(0.5, __dmul_rn(q, 0x1p-51))
-                            : fabs(__dsub_rn(q, d)) == 0.5);
+                bad |= !(q < 0x1p52) || fabs(__dsub_rn(q, d)) == 0.5;
                 const uint64_t tb = sg_bits(t);
                 slo += (uint32_t)tb & 0x3ffffffu;
                 shi += (uint32_t)(tb >> 26) & 0x3ffffffu;
@@ -595,11 +583,6 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
 
         /* general case, one half after the other */
         if (!stepped) {
-            if (HYB) {
-#pragma unroll
-                for (int h = 0; h < G; h++)
-                    e[h] = SG_EXP_NEG(-pmv[h], etab);
-            }
 #pragma unroll
             for (int h = 0; h < G; h++) {
                 if (done)
@@ -686,7 +669,7 @@ __device__ __forceinline__ SgLineResult sg_decode_line(double llr, const SgLineP
         }
         p0 = __dadd_rn(p0, __dmul_rn(pnlc, pp0));
         p1 = __dadd_rn(p1, __dmul_rn(pnlc, pp1));
-        const double lg = SG_LOG(fmax(act ? p0 : p1, 1e-40), ltab);
+        const double lg = sg_dec_log<CR>(fmax(act ? p0 : p1, 1e-40), ltab);
         lapp = __dsub_rn(lg, __shfl_sync(SG_FULL, lg, (lane & 15) + 16));
         le = __dsub_rn(lapp, x);
     }

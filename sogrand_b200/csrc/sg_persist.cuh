@@ -139,7 +139,7 @@ __device__ __forceinline__ void sg_slot_admit(SgSlot& sl, const SgDecodeArgs& ar
     }
 }
 
-template <int NW, int C, int G>
+template <int NW, int C, int G, bool CR>
 __global__ void __launch_bounds__(NW * 32, 1) sg_persist_kernel(const __grid_constant__ SgDecodeArgs args,
                                                                 SgQueue* q)
 {
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(NW * 32, 1) sg_persist_kernel(const __grid_con
         double v = 1.0;
         if (lane < 16) /* L_ch + (alpha*L_E) */
             v = __dadd_rn(__ldg(g + pos), __dmul_rn(alpha, sl.le[pos]));
-        const SgLineResult r = sg_decode_line<G>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+        const SgLineResult r = sg_decode_line<G, false, CR>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
         if (lane < 16) {
             sl.le[pos] = r.le;
             if (args.lapp)

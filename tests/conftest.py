@@ -34,15 +34,17 @@ def kat():
 
 @pytest.fixture(scope="session")
 def oracle_paths():
-    """The CPU checkers (built from oracle/ if missing).  "crq" (the
-    binary128 checker, needs libquadmath) is None where it cannot be built."""
+    """The CPU checkers (built from oracle/ if missing): "libm" (glibc
+    exp/log), "twin" and "twin_cr" (the decoder's table-driven and correctly
+    rounded exp/log); "crq" (the binary128 checker, needs libquadmath) is
+    None where it cannot be built."""
     d = os.path.join(ROOT, "oracle")
-    _ensure_built(d, ["libsg_oracle.so", "libsg_oracle_twin.so"])
+    _ensure_built(d, ["libsg_oracle.so", "libsg_oracle_twin.so", "libsg_oracle_twin_cr.so"])
     crq = os.path.join(d, "libsg_oracle_crq.so")
     if not os.path.exists(crq):
         subprocess.run(["make", "-C", d, "crq"], capture_output=True)
     return {"libm": os.path.join(d, "libsg_oracle.so"), "twin": os.path.join(d, "libsg_oracle_twin.so"),
-            "crq": crq if os.path.exists(crq) else None}
+            "twin_cr": os.path.join(d, "libsg_oracle_twin_cr.so"), "crq": crq if os.path.exists(crq) else None}
 
 
 @pytest.fixture(scope="session")
@@ -59,3 +61,13 @@ def cuda():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return torch
+
+
+@pytest.fixture
+def cr_mode(sg):
+    """The decoder's reference-exact math mode (correctly rounded exp/log)
+    for one test."""
+    old = sg.get_math_mode()
+    sg.set_math_mode(1)
+    yield
+    sg.set_math_mode(old)

@@ -1,11 +1,14 @@
-"""GPU parity: the CUDA decoder, called through the C ABI, against
-  - "ref_cr": the unmodified reference source (SOGRAND_C/cubic_decoder_final.c)
-    compiled against a correctly rounded exp/log -- every value bit for bit:
-    decoded bits, per-codeword iterations, NG, NG_p, convergence and the final
-    L_APP bytes (the decoder's exp/log are correctly rounded too);
-  - "ref": the same source with the system libm (glibc), whose exp/log are
-    not correctly rounded: equal wherever glibc's last bits do not move a
-    discrete decision, and the fixtures record the codewords where they do.
+"""GPU parity: the CUDA decoder, called through the C ABI, against the
+reference SOGRAND_C/cubic_decoder_final.c built from its own sources:
+  - default math mode (table-driven exp/log): every value bit for bit --
+    decoded bits, per-codeword iterations, NG, NG_p, convergence and the
+    final L_APP bytes -- equals the oracle restatement with the same
+    exp/log ("twin"), and the glibc-linked reference ("ref") on every
+    codeword but the recorded ones, where the last bits of glibc's or the
+    table routines' exp/log move a discrete decision;
+  - reference-exact math mode (correctly rounded exp/log): every value bit
+    for bit equals the unmodified reference compiled against a correctly
+    rounded libm ("ref_cr").
 Fixtures: tests/golden/ (generated by make_golden.py and
 make_golden_large.py from the reference)."""
 import hashlib
@@ -38,31 +41,44 @@ def _rec(d, i):
     return d["bits"][i], d["iterations"][i], d["ng"][i], d["ng_p"][i], d["converged"][i]
 
 
-@pytest.mark.parametrize("name", SETS)
-def test_decode_matches_reference(cuda, sg, golden, name):
-    e = golden["sets"][name]
+def _check_set(sg, e, name, target):
+    """Decode a fixture set; compare with `target` ("twin" or "ref_cr") bit
+    for bit, and with the glibc-linked reference except on the recorded
+    codewords."""
     info, llr = _inputs(sg, e)
     assert _sha(llr) == e["llr_sha256"]
     bits, stats, lapp = sg.decode(llr, sg.params(Tmax=e["Tmax"]), want_lapp=True)
     n = e["n_cw"]
-    cr, r, t = e["ref_cr"], e["ref"], e["twin"]
+    want, r = e[target], e["ref"]
     for i in range(n):
         got = (bits[i].tobytes().hex(), float(stats["iterations"][i]), int(stats["ng"][i]),
                int(stats["ng_p"][i]), int(stats["converged"][i]))
         # a codeword with a line that lists no codeword under the Tmax cap
         # is undefined in the reference (it reads an uninitialised list
-        # size); the restatement's defined behaviour is the target there
-        want = t if cr["undefined_lines"][i] else cr
+        # size); the restatements' defined behaviour there is checked
+        # against the live oracles by the Tmax tests below
+        if target == "ref_cr" and e["ref_cr"]["undefined_lines"][i]:
+            continue
         assert got == _rec(want, i), (name, i)
         assert _sha(lapp[i]) == want["lapp_sha256"][i], (name, i)
-    # the glibc-linked reference: equal except on the recorded codewords
-    differ = [i for i in range(n) if _rec(r, i) != _rec(cr, i)]
-    assert len(differ) == e["glibc_vs_cr_mismatches"]
+    count = "glibc_vs_cr_mismatches" if target == "ref_cr" else "glibc_vs_twin_mismatches"
+    differ = [i for i in range(n) if not r["undefined_lines"][i] and _rec(r, i) != _rec(want, i)]
+    assert len(differ) == e[count]
     for i in range(n):
         if i not in differ and not r["undefined_lines"][i]:
             assert bits[i].tobytes().hex() == r["bits"][i]
             assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i])) == \
                 (r["iterations"][i], r["ng"][i], r["ng_p"][i])
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_decode_matches_twin_and_reference(cuda, sg, golden, name):
+    _check_set(sg, golden["sets"][name], name, "twin")
+
+
+@pytest.mark.parametrize("name", SETS)
+def test_reference_exact_mode_matches_reference(cuda, sg, golden, cr_mode, name):
+    _check_set(sg, golden["sets"][name], name, "ref_cr")
 
 
 def test_config1_bits_and_iterations_equal_reference(cuda, sg, golden):
@@ -76,56 +92,85 @@ def test_config1_bits_and_iterations_equal_reference(cuda, sg, golden):
     assert [b.tobytes().hex() for b in bits] == r["bits"]
     assert list(stats["iterations"]) == r["iterations"]
     ng_diff = [i for i in range(100) if int(stats["ng"][i]) != r["ng"][i]]
-    assert len(ng_diff) == e["glibc_vs_cr_mismatches"]
+    assert len(ng_diff) == e["glibc_vs_twin_mismatches"]
 
 
-def test_large_reference_sets(cuda, sg):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_large_reference_sets(cuda, sg, mode):
     """4096 codewords at 2.0 dB and 4096 at 1.5 dB decoded by the reference
-    (tests/golden/golden_large.npz): every codeword equals the reference
-    under a correctly rounded libm, and the glibc-linked reference except on
-    the recorded codewords."""
+    (tests/golden/golden_large.npz): every codeword equals the table-math
+    restatement (math mode 0) or the reference under a correctly rounded
+    libm (math mode 1), and the glibc-linked reference except on the
+    recorded codewords."""
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_large.npz")
     z = np.load(path)
-    for name in ("large_2.0dB", "large_1.5dB"):
-        seed, n = (int(v) for v in z[f"{name}/meta"])
-        _, llr = sg.gen_llr(seed, 0, n, ebn0_db=float(z[f"{name}/ebn0_db"]))
-        assert _sha(llr) == str(z[f"{name}/llr_sha256"])
-        bits, stats, _ = sg.decode(llr)
-        refbits = z[f"{name}/ref_bits"]
-        crbits = refbits.copy()
-        crbits[z[f"{name}/ref_cr_bits_diff_idx"]] = z[f"{name}/ref_cr_bits_diff"]
-        assert np.array_equal(bits, crbits), name
-        for f in ("iterations", "ng", "ng_p", "converged"):
-            assert np.array_equal(stats[f], z[f"{name}/ref_cr_{f}"].astype(stats[f].dtype)), (name, f)
-        differ = (bits != refbits).any(axis=1)
-        for f in ("iterations", "ng", "ng_p", "converged"):
-            differ |= stats[f] != z[f"{name}/ref_{f}"].astype(stats[f].dtype)
-        assert np.array_equal(np.flatnonzero(differ), z[f"{name}/ref_vs_ref_cr_idx"]), name
+    target = "twin" if mode == 0 else "ref_cr"
+    old = sg.get_math_mode()
+    sg.set_math_mode(mode)
+    try:
+        for name in ("large_2.0dB", "large_1.5dB"):
+            seed, n = (int(v) for v in z[f"{name}/meta"])
+            _, llr = sg.gen_llr(seed, 0, n, ebn0_db=float(z[f"{name}/ebn0_db"]))
+            assert _sha(llr) == str(z[f"{name}/llr_sha256"])
+            bits, stats, _ = sg.decode(llr)
+            refbits = z[f"{name}/ref_bits"]
+            want = refbits.copy()
+            want[z[f"{name}/{target}_bits_diff_idx"]] = z[f"{name}/{target}_bits_diff"]
+            assert np.array_equal(bits, want), name
+            for f in ("iterations", "ng", "ng_p", "converged"):
+                assert np.array_equal(stats[f], z[f"{name}/{target}_{f}"].astype(stats[f].dtype)), (name, f)
+            differ = (bits != refbits).any(axis=1)
+            for f in ("iterations", "ng", "ng_p", "converged"):
+                differ |= stats[f] != z[f"{name}/ref_{f}"].astype(stats[f].dtype)
+            assert np.array_equal(np.flatnonzero(differ), z[f"{name}/ref_vs_{target}_idx"]), name
+    finally:
+        sg.set_math_mode(old)
 
 
-@pytest.mark.parametrize("tag,L,tmax", [("L3", 3, UINT64_MAX), ("L1", 1, UINT64_MAX), ("L4", 4, UINT64_MAX),
-                                        ("T10", 3, 10), ("T100", 3, 100), ("T1000", 3, 1000)])
-def test_line_kats(cuda, sg, kat, tag, L, tmax):
+KATS = [("L3", 3, UINT64_MAX), ("L1", 1, UINT64_MAX), ("L4", 4, UINT64_MAX), ("T10", 3, 10), ("T100", 3, 100),
+        ("T1000", 3, 1000)]
+
+
+def _undefined(kat, tag, n):
+    return kat[f"{tag}_undefined"].astype(bool) if f"{tag}_undefined" in kat else np.zeros(n, bool)
+
+
+@pytest.mark.parametrize("tag,L,tmax", KATS)
+def test_line_kats(cuda, sg, kat, oracle_paths, tag, L, tmax):
     """SOGRAND_bitSO on 528 lines (incl. ties, zeros, equal magnitudes, huge
     IC, saturated reliabilities), with and without a Tmax cap: guess counts
-    equal the reference's; L_APP and L_E equal, byte for byte, those of the
-    reference under a correctly rounded libm.  Lines that list no codeword
-    under the cap are undefined in the reference beyond N_guess; the decoder
+    and signs equal the glibc-linked reference's; soft values equal the
+    table-math restatement bit for bit.  Lines that list no codeword under
+    the cap are undefined in the reference beyond N_guess; the decoder
     returns L_APP = input, L_E = 0 there (the reference's curL == 0 branch)."""
     lapp, le, ng, nc = sg.bitso(kat["llr"], L=L, Tmax=tmax)
+    assert np.array_equal(ng, kat[f"{tag}_nguess"])
+    undef = _undefined(kat, tag, len(ng))
+    assert np.array_equal(nc == 0, undef)
+    d = ~undef
+    assert np.array_equal(lapp[d] > 0, kat[f"{tag}_lapp"][d] > 0)
+    assert np.array_equal(lapp[undef].view(np.int64), kat["llr"][undef].view(np.int64))
+    assert not le[undef].any()
+    tl, te, tn, _ = Oracle(oracle_paths["twin"]).bitso(kat["llr"], L=L, Tmax=tmax)
+    assert np.array_equal(ng, tn)
+    assert np.array_equal(lapp.view(np.int64), tl.view(np.int64))
+    assert np.array_equal(le.view(np.int64), te.view(np.int64))
+    err = np.abs(lapp[d] - kat[f"{tag}_lapp"][d])
+    print(f"{tag}: max |L_APP - glibc reference| = {err.max():.3g}")
+
+
+@pytest.mark.parametrize("tag,L,tmax", KATS)
+def test_line_kats_reference_exact(cuda, sg, kat, cr_mode, tag, L, tmax):
+    """The same lines in the reference-exact math mode: L_APP and L_E equal,
+    byte for byte, those of the reference under a correctly rounded libm."""
+    lapp, le, ng, nc = sg.bitso(kat["llr"], L=L, Tmax=tmax)
     assert np.array_equal(ng, kat[f"{tag}_cr_nguess"])
-    undef = kat[f"{tag}_cr_undefined"].astype(bool) if f"{tag}_cr_undefined" in kat else np.zeros(len(ng), bool)
+    undef = _undefined(kat, tag + "_cr", len(ng))
     assert np.array_equal(nc == 0, undef)
     d = ~undef
     assert np.array_equal(lapp[d].view(np.int64), kat[f"{tag}_cr_lapp"][d].view(np.int64))
     assert np.array_equal(le[d].view(np.int64), kat[f"{tag}_cr_le"][d].view(np.int64))
     assert np.array_equal(lapp[undef].view(np.int64), kat["llr"][undef].view(np.int64))
-    assert not le[undef].any()
-    # the glibc-linked reference: same guess counts and signs
-    assert np.array_equal(ng, kat[f"{tag}_nguess"])
-    assert np.array_equal(lapp[d] > 0, kat[f"{tag}_lapp"][d] > 0)
-    err = np.abs(lapp[d] - kat[f"{tag}_lapp"][d])
-    print(f"{tag}: max |L_APP - glibc reference| = {err.max():.3g}")
 
 
 @pytest.mark.parametrize("tmax", [1, 2, 10, 100, 1000, 0])
@@ -176,3 +221,26 @@ def test_random_mixed_codewords_match_twin(cuda, sg, oracle_paths):
             assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i]),
                     int(stats["converged"][i]), int(stats["phases"][i])) == ts, i
             assert np.array_equal(lapp[i].view(np.int64), tl.view(np.int64)), i
+
+
+def test_random_codewords_reference_exact_mode(cuda, sg, oracle_paths, cr_mode):
+    """64 fresh codewords at per-codeword Eb/N0 ~ U[1, 3] dB in the
+    reference-exact math mode, through the batched and the plain decoder:
+    bits, statistics and L_APP bytes equal the restatement with the same
+    correctly rounded exp/log, with and without a Tmax cap."""
+    torch = cuda
+    n = 64
+    _, llr = sg.gen_llr(4244, 0, n, ebn0_range=(1.0, 3.0))
+    for kw in ({}, {"Tmax": 1000}):
+        with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+            ref = pool.map(twin_decode_one, [(oracle_paths["twin_cr"], llr[i], kw) for i in range(n)])
+        hb, hs, hl = sg.decode(llr, sg.params(**kw), want_lapp=True)
+        db, draw, dl = sg.decode(torch.from_numpy(llr).cuda(), sg.params(**kw), want_lapp=True)
+        torch.cuda.synchronize()
+        ds, db, dl = sg.stats_from_device(draw), db.cpu().numpy(), dl.cpu().numpy()
+        for bits, stats, lapp in ((hb, hs, hl), (db, ds, dl)):
+            for i, (tb, ts, tl) in enumerate(ref):
+                assert np.array_equal(bits[i], tb), i
+                assert (stats["iterations"][i], int(stats["ng"][i]), int(stats["ng_p"][i]),
+                        int(stats["converged"][i]), int(stats["phases"][i])) == ts, i
+                assert np.array_equal(lapp[i].view(np.int64), tl.view(np.int64)), i

@@ -1,14 +1,15 @@
 """The decoder's exp and log.
 
-The kernel and the twin oracle evaluate exp/log with the correctly rounded
-routines of sogrand_b200/csrc/sg_crmath.h (the same source on host and
-device).  They are checked here on the host, through the twin oracle,
+In its reference-exact mode the kernel evaluates exp/log with the correctly
+rounded routines of sogrand_b200/csrc/sg_crmath.h (the same source on host
+and device, built into the twin_cr oracle).  They are checked here on the
+host, through that oracle,
 against two independent references: mpmath at 200 bits, and the binary128
 checker of oracle/crq.h (libsg_oracle_crq.so) on large samples, on the
 structured arguments the decoder produces (1 +- m 2^-52: JacLog of large
 |LLR|), on subnormal and overflow boundaries, and with the slow paths forced.
-The table-driven routines of sg_math.h, which the input generator uses, are
-checked for their 0.51 ulp bound."""
+The table-driven routines of sg_math.h -- the default decoder's, and the
+input generator's -- are checked for their 0.51 ulp bound."""
 import ctypes as C
 
 import numpy as np
@@ -26,7 +27,7 @@ def _ulp_err(y, y_exact):
 
 @pytest.fixture(scope="module")
 def twin(oracle_paths):
-    o = Oracle(oracle_paths["twin"])
+    o = Oracle(oracle_paths["twin_cr"])
     for name in ("sgo_exp_cr_slow", "sgo_log_cr_slow", "sgo_exp_tab", "sgo_log_tab"):
         f = getattr(o.lib, name)
         f.restype = C.c_double
@@ -135,7 +136,7 @@ def test_special_values(twin):
 
 
 def test_table_routines_accuracy(twin):
-    """sg_math.h's table-driven exp/log (the input generator's): < 0.51 ulp."""
+    """sg_math.h's table-driven exp/log: < 0.51 ulp."""
     import mpmath as mp
 
     mp.mp.prec = 120
@@ -152,8 +153,8 @@ def test_table_routines_accuracy(twin):
 
 def test_agreement_with_glibc(twin, libm):
     """glibc's exp/log (the reference's libm here) are not correctly rounded:
-    they differ from the decoder's by one ulp on a small fraction of
-    arguments, never more."""
+    they differ from the correctly rounded ones by one ulp on a small
+    fraction of arguments, never more."""
     rng = np.random.default_rng(11)
     xs = rng.uniform(-50, 50, 20000)
     a = np.array([twin.lib.sgo_exp(float(x)) for x in xs])

@@ -47,10 +47,22 @@ def test_oracle_line_kats_bit_exact(libm, kat, tag, L, tmax):
 
 
 @pytest.mark.parametrize("tag,L,tmax", KATS)
-def test_twin_line_kats_bit_exact(twin, kat, tag, L, tmax):
-    """The twin (the decoder's correctly rounded exp/log) reproduces the
-    reference compiled against a correctly rounded libm."""
-    _kat_check(twin, kat, tag + "_cr", L, tmax)
+def test_twin_cr_line_kats_bit_exact(oracle_paths, kat, tag, L, tmax):
+    """The restatement with the decoder's correctly rounded exp/log
+    reproduces the reference compiled against a correctly rounded libm."""
+    _kat_check(Oracle(oracle_paths["twin_cr"]), kat, tag + "_cr", L, tmax)
+
+
+@pytest.mark.parametrize("tag,L,tmax", KATS)
+def test_twin_line_kats_discrete(twin, kat, tag, L, tmax):
+    """The restatement with the default, table-driven exp/log: the glibc
+    reference's guess counts and signs; soft values within 1e-6."""
+    lapp, le, ng, nc = twin.bitso(kat["llr"], L=L, Tmax=tmax)
+    assert np.array_equal(ng, kat[f"{tag}_nguess"])
+    undef = kat[f"{tag}_undefined"].astype(bool) if f"{tag}_undefined" in kat else np.zeros(len(ng), bool)
+    d = ~undef
+    assert np.array_equal(lapp[d] > 0, kat[f"{tag}_lapp"][d] > 0)
+    assert np.abs(lapp[d] - kat[f"{tag}_lapp"][d]).max() < 1e-6
 
 
 def test_fixture_inputs_regenerate(sg, golden):
@@ -79,23 +91,20 @@ def test_oracle_codewords_match_reference(sg, golden, oracle_paths):
         assert hashlib.sha256(lapp.tobytes()).hexdigest() == r["lapp_sha256"][i]
 
 
-def test_reference_glibc_vs_correctly_rounded(golden):
-    """The reference under glibc and under a correctly rounded libm differ
-    only where glibc's last bits move a discrete decision; the fixtures
-    record how often, and the decoded bits at 2 dB never differ.  The twin
-    equals the correctly rounded build in every recorded value."""
+def test_reference_glibc_vs_restatements(golden):
+    """The reference under glibc differs from it under a correctly rounded
+    libm, and from the table-math restatement, only where last bits of
+    exp/log move a discrete decision; the fixtures record how often, and the
+    decoded bits at 2 dB never differ."""
+    keys = ("bits", "iterations", "ng", "ng_p", "converged")
     for name, e in golden["sets"].items():
         r, cr, t = e["ref"], e["ref_cr"], e["twin"]
-        diff = [i for i in range(e["n_cw"]) if (r["bits"][i], r["iterations"][i], r["ng"][i], r["ng_p"][i],
-                                                  r["converged"][i])
-                != (cr["bits"][i], cr["iterations"][i], cr["ng"][i], cr["ng_p"][i], cr["converged"][i])]
-        assert len(diff) == e["glibc_vs_cr_mismatches"], name
-        for i in range(e["n_cw"]):
-            if not cr["undefined_lines"][i]:
-                for f in ("bits", "iterations", "ng", "ng_p", "converged", "lapp_sha256"):
-                    assert t[f][i] == cr[f][i], (name, i, f)
+        for other, count in ((cr, "glibc_vs_cr_mismatches"), (t, "glibc_vs_twin_mismatches")):
+            diff = [i for i in range(e["n_cw"]) if not r["undefined_lines"][i]
+                    and tuple(r[k][i] for k in keys) != tuple(other[k][i] for k in keys)]
+            assert len(diff) == e[count], (name, count)
     e = golden["sets"]["cfg1_2dB_100"]
-    assert e["ref"]["bits"] == e["ref_cr"]["bits"]
+    assert e["ref"]["bits"] == e["ref_cr"]["bits"] == e["twin"]["bits"]
 
 
 def test_early_termination_oracle(libm, sg):
