@@ -229,19 +229,31 @@ _REF_LIB = None
 def _ref_harness_decode(args):
     """Pool worker: one codeword through the reference's own functions
     (oracle/_ref/libsgref.so, glibc libm) at the given Tmax; returns the
-    packed bits."""
+    packed bits and whether a line decode read the reference's
+    uninitialised list size (possible only under a finite Tmax; the
+    reference's output is undefined then).  The check runs each line's
+    search once more, so it is done only when Tmax is finite."""
     global _REF_LIB
     llr, tmax = args
     if _REF_LIB is None:
         _REF_LIB = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libsgref.so"))
         dp = np.ctypeslib.ndpointer(np.float64, flags="C")
         u8 = np.ctypeslib.ndpointer(np.uint8, flags="C")
+        i32 = np.ctypeslib.ndpointer(np.int32, flags="C")
         _REF_LIB.sgref_decode.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp, u8,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _REF_LIB.sgref_decode_checked.argtypes = [dp, C.c_size_t, C.c_int, C.c_int, C.c_uint64, C.c_double, dp,
+                                                  u8, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  i32]
     bits = np.zeros(64, np.uint8)
-    _REF_LIB.sgref_decode(np.ascontiguousarray(llr), 1, 3, 30, tmax, 1.0 - 1e-5, np.full(100, 0.7), bits, None,
-                          None, None, None, None)
-    return bits
+    und = np.zeros(1, np.int32)
+    if tmax == (1 << 64) - 1:
+        _REF_LIB.sgref_decode(np.ascontiguousarray(llr), 1, 3, 30, tmax, 1.0 - 1e-5, np.full(100, 0.7), bits,
+                              None, None, None, None, None)
+    else:
+        _REF_LIB.sgref_decode_checked(np.ascontiguousarray(llr), 1, 3, 30, tmax, 1.0 - 1e-5, np.full(100, 0.7),
+                                      bits, None, None, None, None, None, und)
+    return bits, int(und[0])
 
 
 def run_sweep(args):
@@ -275,20 +287,83 @@ def run_sweep(args):
                     _, llr = sg.gen_llr(args.seed, 0, n_cpu, ebn0_db=eb)
                     gbits, _, _ = sg.decode(llr, p)
                     t0 = time.perf_counter()
-                    rbits = pool.map(_ref_harness_decode, [(llr[i], tmax) for i in range(n_cpu)], chunksize=1)
+                    res = pool.map(_ref_harness_decode, [(llr[i], tmax) for i in range(n_cpu)], chunksize=1)
                     dt = time.perf_counter() - t0
+                    und = [r[1] > 0 for r in res]
                     row["cpu_reference"] = {
                         "codewords_per_s": n_cpu / dt, "codewords": n_cpu, "cores": cores,
                         "how": "reference functions (oracle/_ref/libsgref.so, -O2, glibc), one codeword per "
-                               "task from a shared queue over all host cores",
-                        "bits_differing_from_gpu": int(sum(not np.array_equal(a, b) for a, b in zip(rbits, gbits)))}
+                               "task from a shared queue over all host cores"
+                               + ("" if tmax == (1 << 64) - 1 else "; each line's search run twice to detect "
+                                  "the reference's undefined (uninitialised list size) lines, so the rate is "
+                                  "understated"),
+                        "codewords_undefined_in_reference": int(sum(und)),
+                        "defined_codewords_with_bits_differing_from_gpu": int(sum(
+                            not np.array_equal(r[0], b) for r, b, u in zip(res, gbits, und) if not u))}
                 rows.append(row)
                 c = row.get("cpu_reference", {})
                 print(f"Tmax {row['tmax']:>5} {eb:5.2f} dB  GPU {row['codewords_per_s']:9.0f} cw/s  "
                       f"BER {row['ber']:.3e}  it {row['avg_iterations']:5.2f}  NG {row['ng_per_codeword']:9.0f}  "
-                      f"CPU {c.get('codewords_per_s', 0):7.2f} cw/s ({c.get('bits_differing_from_gpu')})",
-                      flush=True)
+                      f"CPU {c.get('codewords_per_s', 0):7.2f} cw/s (undefined {c.get('codewords_undefined_in_reference')}, "
+                      f"differing {c.get('defined_codewords_with_bits_differing_from_gpu')})", flush=True)
     print(json.dumps({"sweep": rows}), flush=True)
+
+
+def run_ref_gpu(args):
+    """The reference's own GPU decoder (SOGRAND_CUDA/cubic_decoder1.cu built
+    unmodified for sm_100a into oracle/_ref) on this GPU, beside this
+    library on the same codewords: the first n codewords of the bench
+    stream at 2 dB as one LLR file.  Reports both decoders' device-timed
+    codewords/s (the reference's own "Total GPU time" line, which brackets
+    its kernel launches with CUDA events; this library's sg_decode_device
+    with CUDA events) and how many codewords' decoded bits differ."""
+    import torch
+
+    import sogrand_b200 as sg
+    from sogrand_b200 import autotune
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "cubic_decoder1_sm100a")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "oracle/_ref/cubic_decoder1_sm100a not built"}))
+        return
+    n = args.ref_gpu_cw
+    _, llr = sg.gen_llr(SEED, 0, n, ebn0_db=EBN0)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "llr.bin"), os.path.join(td, "dec.bin")
+        llr.tofile(fin)
+        t0 = time.perf_counter()
+        out = subprocess.run([exe, fin, fout], capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+        if out.returncode != 0:
+            print(json.dumps({"impl": "reference_gpu", "unavailable": f"exit {out.returncode}: "
+                              + out.stderr.strip()[-200:]}))
+            return
+        lines = {l.split(":")[0].strip(): l.split(":", 1)[1].strip() for l in out.stdout.splitlines() if ":" in l}
+        ref_bits = np.fromfile(fout, np.uint8).reshape(n, 64)
+    gpu_s = float(lines["Total GPU time"].split()[0])
+    torch.cuda.set_device(0)
+    d = torch.from_numpy(llr).cuda()
+    sg.decode(d)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    bits, _, _ = sg.decode(d)
+    e1.record()
+    torch.cuda.synchronize()
+    ours = e0.elapsed_time(e1) / 1000.0
+    bits = bits.cpu().numpy()
+    print(json.dumps({
+        "impl": "reference_gpu", "codewords": n, "ebn0_db": EBN0,
+        "reference_gpu": {"codewords_per_s": n / gpu_s, "gpu_seconds": gpu_s, "process_wall_s": wall,
+                          "avg_iterations": float(lines["Average iterations per block"]),
+                          "avg_ng": float(lines["Average NG per block"]),
+                          "build": "SOGRAND_CUDA/cubic_decoder1.cu, nvcc -O3 -use_fast_math, sm_100a"},
+        "this_library": {"codewords_per_s": n / ours, "gpu_seconds": ours, "api": "sg_decode_device",
+                         "variant": autotune.get_variant()},
+        "speedup": gpu_s / ours,
+        "codewords_with_different_bits": int((ref_bits != bits).any(axis=1).sum()),
+        "note": "the reference GPU decoder swaps the C decoder's first two phase axes and uses CUDA's "
+                "exp/log with FMA contraction, so its results may differ from the C reference's"}), flush=True)
 
 
 def bench_config(args, n, world):
@@ -323,6 +398,11 @@ def main():
     ap.add_argument("--ebn0", default="1.0:3.0:0.25", help="sweep points, a:b:step or a comma list (dB)")
     ap.add_argument("--tmax", default="inf,1000", help="sweep Tmax values, comma list ('inf' = none)")
     ap.add_argument("--seed", type=int, default=20261203, help="sweep stream seed")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="instead of the bench line: the reference's own GPU decoder beside this library")
+    ap.add_argument("--ref-gpu-cw", type=int, default=1000)
+    ap.add_argument("--math", type=int, default=0, choices=[0, 1],
+                    help="math mode: 0 table-driven exp/log, 1 correctly rounded (reference-exact)")
     ap.add_argument("--port-worker", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.port_worker:
@@ -330,6 +410,9 @@ def main():
         return
     if args.sweep:
         run_sweep(args)
+        return
+    if args.ref_gpu:
+        run_ref_gpu(args)
         return
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -354,6 +437,8 @@ def main():
     from sogrand_b200 import autotune
 
     from sogrand_b200 import batch as B
+
+    sg.set_math_mode(args.math)
 
     tune = None
     snr_kw = dict(ebn0_db=EBN0) if args.workload == "2dB" else dict(ebn0_range=(1.0, 3.0))
@@ -435,9 +520,9 @@ def main():
                "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
                "api": "sg_decode_host (host buffers, copies inside the timed region)"}
 
-    ceil, ceil_tab = C.c_double(), C.c_double()
-    _lib.check(lib.sg_guess_ceiling(20000, 0, C.byref(ceil)))
-    _lib.check(lib.sg_guess_ceiling(20000, 1, C.byref(ceil_tab)))
+    ceil, ceil_other = C.c_double(), C.c_double()
+    _lib.check(lib.sg_guess_ceiling(20000, args.math, C.byref(ceil)))
+    _lib.check(lib.sg_guess_ceiling(20000, 1 - args.math, C.byref(ceil_other)))
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -461,10 +546,10 @@ def main():
                               "peak": ceil.value, "unit": "guess/s per GPU",
                               "frac": value * ng_per_cw / world / ceil.value,
                               "how": "sg_guess_ceiling: PM add + exp(-PM) + P_notGuess subtract per guess, "
-                                     "all SMs, measured on this GPU in this run, with the decoder's correctly "
-                                     "rounded exp",
-                              "peak_table_exp": ceil_tab.value,
-                              "frac_table_exp": value * ng_per_cw / world / ceil_tab.value},
+                                     "all SMs, measured on this GPU in this run, with the exp of the math "
+                                     "mode used (" + ("table-driven" if args.math == 0 else "correctly rounded")
+                                     + ")",
+                              "peak_other_math_mode": ceil_other.value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": DRAM_BYTES_PER_CW[args.form] * n,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of 2368 codewords "
@@ -472,6 +557,8 @@ def main():
                          "note": f"peak {peak_src}; the decoder is FP64/issue-bound, see guesses_per_s"},
             "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
             "form": args.form, "autotune": tune,
+            "math_mode": ("table-driven exp/log (default)" if args.math == 0 else
+                          "correctly rounded exp/log (reference-exact)"),
             "variant": B.get_variant() if args.form == "batch" else autotune.get_variant(),
         }
         if not args.no_cpu_baseline:

@@ -301,9 +301,11 @@ sg_status sg_set_math_mode(int32_t mode);
 int32_t sg_get_math_mode(void);
 
 /* ---- kernel configuration (process-wide).  Variants differ in warps per
- * codeword CTA and in where the 32 KB channel cube is held (shared memory,
- * staged by a bulk asynchronous copy, or global memory through L2); all give
- * identical results.  sogrand_b200.autotune() measures them. */
+ * codeword CTA, in where the 32 KB channel cube is held (shared memory,
+ * staged by a bulk asynchronous copy, or global memory through L2) and in
+ * error patterns per lane; all give identical results.
+ * sogrand_b200.autotune() measures them.  The selection is kept per math
+ * mode: the setters change the current mode's. */
 int sg_decoder_variant_count(void);
 const char* sg_decoder_variant_name(int v);
 sg_status sg_decoder_set_variant(int v);

@@ -655,8 +655,15 @@ struct DevCtx {
 std::mutex g_mu;
 std::atomic<long long> g_wait_limit{SG_WAIT_LIMIT_DEFAULT};
 std::atomic<int> g_math_mode{0}; /* 0: table-driven exp/log, 1: correctly rounded */
-int g_pvariant = 5; /* p32x3-g2: fastest on B200 (sogrand_b200.autotune.autotune_batch) */
-int g_variant = 4; /* w16-gmem-g2: fastest on B200 at 2 dB (sogrand_b200.autotune) */
+/* Selected kernel variants, one per math mode (sogrand_b200.autotune
+ * measures them): on B200 at 2 dB the table math is fastest with two error
+ * patterns per lane (p32x3-g2, w16-gmem-g2), the correctly rounded math,
+ * whose larger exp leaves no registers for the second pattern, with one
+ * (p32x3, w16-gmem). */
+int g_pvariant_by_mode[2] = {5, 4};
+int g_variant_by_mode[2] = {4, 3};
+#define g_pvariant (g_pvariant_by_mode[g_math_mode.load()])
+#define g_variant (g_variant_by_mode[g_math_mode.load()])
 DevCtx g_ctx[64];
 std::vector<uint32_t> g_enum_host;
 sg_code_tables g_code;

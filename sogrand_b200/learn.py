@@ -112,6 +112,8 @@ def main():
     ap.add_argument("--eval-ebn0", default="1.25,1.5,1.75,2.0")
     ap.add_argument("--eval-cw", type=int, default=500000)
     ap.add_argument("--eval-imax", default="5,10,30")
+    ap.add_argument("--no-plain-same-imax", action="store_true",
+                    help="compare only against the plain decoder at Imax 30")
     ap.add_argument("--seed", type=int, default=90210)
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
@@ -140,10 +142,10 @@ def main():
     for im in imaxes:
         configs[f"learned{im}"] = (alpha, im)
         pairs.append((f"learned{im}", "plain30"))
-        if im != 30:
+        if im != 30 and not args.no_plain_same_imax:
             configs[f"plain{im}"] = (None, im)
             pairs.append((f"learned{im}", f"plain{im}"))
-    for eb in [float(x) for x in args.eval_ebn0.split(",")]:
+    for eb in [float(x) for x in args.eval_ebn0.split(",") if x.strip()]:
         row = evaluate_set(configs, eb, args.eval_cw, eval_seed, 0, pairs=pairs)
         res["eval"].append(row)
         print(json.dumps(row), flush=True)
