@@ -69,3 +69,15 @@ def test_mixed_snr_range(sg):
     assert np.isfinite(llr).all()
     spread = [np.mean(np.abs(l)) for l in llr]
     assert max(spread) > 1.2 * min(spread)
+
+
+def test_reference_arm_inputs_equal_library_generator(sg, tmp_path):
+    """The CPU legs of bench.py write their LLR files with the oracle's build
+    of the generator, so the process timing the reference never loads this
+    library; the files must hold exactly the bench stream's codewords."""
+    import bench
+
+    files = bench.ref_inputs(str(tmp_path), 3)
+    _, llr = sg.gen_llr(bench.SEED, 0, 3, ebn0_db=bench.EBN0)
+    for c, f in enumerate(files):
+        assert np.fromfile(f).tobytes() == llr[c].tobytes(), c
