@@ -1,21 +1,22 @@
 """Large reference-pinned fixtures and the glibc / correctly-rounded survey.
 
 Run from the repository root where the reference sources are available
-(after `make -C oracle all crq tab ref REF=<reference root>` and
+(after `make -C oracle all ref REF=<reference root>` and
 `make -C sogrand_b200/csrc`):
 
-    python tests/golden/make_golden_large.py [--procs N] [--kinds ref,ref_cr,tab]
+    python tests/golden/make_golden_large.py [--procs N] [--kinds ref,ref_cr,twin]
 
 For each set below, every codeword is decoded by
   ref     the unmodified reference (oracle/_ref/libsgref.so: the reference's
           SOGRAND_bitSO / early_termination / hard_decision, glibc exp/log),
   ref_cr  the same unmodified source under a correctly rounded exp/log
           (oracle/_ref/libsgref_cr.so) -- the decoder's exact target,
-  tab     the restatement with the table-driven exp/log of sg_math.h
-          (within 0.51 ulp, not correctly rounded; libsg_oracle_tab.so),
+  twin    the restatement with the table-driven exp/log of sg_math.h
+          (within 0.51 ulp, not correctly rounded; libsg_oracle_twin.so),
+          the decoder's default math mode,
 and the discrete results (decoded bits, iterations, NG, NG_p, converged)
 are written to tests/golden/golden_large.npz.  ref and ref_cr differ only
-through glibc's misrounded last bits, tab only through its own, so the count
+through glibc's misrounded last bits, twin only through its own, so the count
 of codewords whose results differ from ref measures what each exp/log
 choice costs in parity with the glibc-linked reference.  Results already in
 the output file for the same inputs (same LLR SHA-256) are reused for kinds
@@ -41,7 +42,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 LIBS = {
     "ref": os.path.join(ROOT, "oracle", "_ref", "libsgref.so"),
     "ref_cr": os.path.join(ROOT, "oracle", "_ref", "libsgref_cr.so"),
-    "tab": os.path.join(ROOT, "oracle", "libsg_oracle_tab.so"),
+    "twin": os.path.join(ROOT, "oracle", "libsg_oracle_twin.so"),
 }
 OUT = os.path.join(ROOT, "tests", "golden", "golden_large.npz")
 UINT64_MAX = (1 << 64) - 1
@@ -95,14 +96,14 @@ def _job(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--procs", type=int, default=max(1, (os.cpu_count() or 2) - 1))
-    ap.add_argument("--kinds", default="ref,ref_cr,tab")
+    ap.add_argument("--kinds", default="ref,ref_cr,twin")
     ap.add_argument("--n-cw", type=int, default=0, help="override the codewords per set (testing the script)")
     ap.add_argument("--out", default=OUT)
     args = ap.parse_args()
     kinds = args.kinds.split(",")
     for k in kinds:
         if not os.path.exists(LIBS[k]):
-            sys.exit(f"missing {LIBS[k]}: run `make -C oracle all crq tab ref REF=...` first")
+            sys.exit(f"missing {LIBS[k]}: run `make -C oracle all ref REF=...` first")
     import sogrand_b200 as sg
 
     old = dict(np.load(args.out)) if os.path.exists(args.out) else {}
@@ -120,7 +121,7 @@ def main():
             out[f"{name}/info_sha256"] = np.array(hashlib.sha256(info.tobytes()).hexdigest())
             same_inputs = str(old.get(f"{name}/llr_sha256", "")) == sha
             full = {}
-            for kind in ("ref", "ref_cr", "tab"):
+            for kind in ("ref", "ref_cr", "twin"):
                 if kind not in kinds:
                     if same_inputs and f"{name}/{kind}_ng" in old:
                         bits = old[f"{name}/ref_bits"].copy()

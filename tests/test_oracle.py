@@ -114,3 +114,34 @@ def test_early_termination_oracle(libm, sg):
     assert libm.lib.sgo_early_termination(np.ascontiguousarray(lapp)) == 1
     lapp[1234] = -lapp[1234]
     assert libm.lib.sgo_early_termination(np.ascontiguousarray(lapp)) == 0
+
+
+def test_large_fixture_pinned_by_restatements(sg, oracle_paths):
+    """golden_large.npz (4096 codewords at 2.0 and 1.5 dB, decoded by the
+    reference, by the reference under a correctly rounded libm, and by the
+    table-math restatement): its inputs regenerate, and on sampled codewords
+    -- every recorded mismatch with the glibc-linked reference among them --
+    the table-math oracle reproduces the twin entries and the correctly
+    rounded oracle the ref_cr entries."""
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_large.npz"))
+    jobs, want = [], []
+    for name in ("large_2.0dB", "large_1.5dB"):
+        seed, n = (int(v) for v in z[f"{name}/meta"])
+        _, llr = sg.gen_llr(seed, 0, n, ebn0_db=float(z[f"{name}/ebn0_db"]))
+        assert hashlib.sha256(llr.tobytes()).hexdigest() == str(z[f"{name}/llr_sha256"]), name
+        for kind, lib in (("twin", "twin"), ("ref_cr", "twin_cr")):
+            bits = z[f"{name}/ref_bits"].copy()
+            bits[z[f"{name}/{kind}_bits_diff_idx"]] = z[f"{name}/{kind}_bits_diff"]
+            idx = sorted(set(z[f"{name}/ref_vs_{kind}_idx"].tolist()) | {0, n - 1})
+            for i in idx:
+                jobs.append((oracle_paths[lib], llr[i], {}))
+                want.append((name, kind, i, bits[i].tobytes(),
+                             tuple(int(z[f"{name}/{kind}_{f}"][i]) for f in ("ng", "ng_p", "converged")),
+                             float(z[f"{name}/{kind}_iterations"][i])))
+    with mp.get_context("spawn").Pool(8) as pool:
+        res = pool.map(twin_decode_one, jobs)
+    for (name, kind, i, b, discrete, it), (bits, st, _) in zip(want, res):
+        assert bits.tobytes() == b, (name, kind, i)
+        assert (st[1], st[2], st[3]) == discrete and st[0] == it, (name, kind, i)
