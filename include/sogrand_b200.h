@@ -302,8 +302,10 @@ int32_t sg_get_math_mode(void);
 
 /* ---- kernel configuration (process-wide).  Variants differ in warps per
  * codeword CTA, in where the 32 KB channel cube is held (shared memory,
- * staged by a bulk asynchronous copy, or global memory through L2) and in
- * error patterns per lane; all give identical results.
+ * staged by a bulk asynchronous copy, or global memory through L2), in
+ * error patterns per lane per step, and in lines per warp (one line on 32
+ * lanes, or two lines on 16 lanes each: the "-l2-" variants); all give
+ * identical results.
  * sogrand_b200.autotune() measures them.  The selection is kept per math
  * mode: the setters change the current mode's. */
 int sg_decoder_variant_count(void);

@@ -1,8 +1,11 @@
 """Autotuner of the decoder's kernel configuration.
 
-Every variant (warps per codeword CTA; channel cube in shared memory or in
-global memory) computes bit-identical results; they differ only in speed,
-which depends on the codeword mix.  autotune() decodes one seeded batch of
+Every variant of the plain decoder computes bit-identical results; they
+differ only in speed, which depends on the codeword mix.  The dimensions:
+warps per codeword CTA (8 to 16); the channel cube in shared memory (staged
+by a bulk copy) or read from global memory; error patterns per lane per step
+(G = 1, 2 or 4); lines per warp (1: 32 lanes per line; 2: 16 lanes per
+line, the "-l2-" variants).  autotune() decodes one seeded batch of
 the caller's workload with each variant, timed with CUDA events, and selects
 the fastest for the process.
 """

@@ -39,6 +39,7 @@
 #include "sg_enum.h"
 #include "sg_gen.h"
 #include "sg_line.cuh"
+#include "sg_line16.cuh"
 #include "sg_math.h"
 
 #define SG_THREADS 256
@@ -111,13 +112,13 @@ __device__ __forceinline__ void sg_cw_not_decoded(const SgDecodeArgs& args, unsi
 /* Shared memory of a decode CTA.  With LCH_SMEM the channel cube is staged
  * here by one bulk copy; otherwise each line reads its 16 channel LLRs from
  * global memory (L2-resident) once per phase. */
-template <int NW, bool LCH_SMEM>
+template <int NW, bool LCH_SMEM, int LPW = 1> /* LPW: lines decoded per warp at a time */
 struct SgCwSmem {
     alignas(16) double lch[LCH_SMEM ? SG_CUBE : 2]; /* bulk-copy destination */
     double le[SG_CUBE];
     alignas(16) double etab[SG_EXP_TAB_LEN]; /* read as double2 by the exp routines */
     alignas(16) double ltab[SG_LOG_TAB_LEN];
-    SgWarpScratch ws[NW];
+    SgWarpScratch ws[NW * LPW];
     uint16_t hdw[256];
     unsigned long long mbar;
     unsigned long long ng;
@@ -179,11 +180,11 @@ __device__ __forceinline__ uint32_t sg_smem_u32(const void* p)
 
 extern __shared__ __align__(128) unsigned char sg_smem_raw[];
 
-template <int NW, bool LCH_SMEM, int MINB, int G, bool CR>
+template <int NW, bool LCH_SMEM, int MINB, int G, bool CR, int LPW = 1>
 __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_constant__ SgDecodeArgs args)
 {
     constexpr int NT = NW * 32;
-    SgCwSmem<NW, LCH_SMEM>& S = *reinterpret_cast<SgCwSmem<NW, LCH_SMEM>*>(sg_smem_raw);
+    SgCwSmem<NW, LCH_SMEM, LPW>& S = *reinterpret_cast<SgCwSmem<NW, LCH_SMEM, LPW>*>(sg_smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool use_bulk = LCH_SMEM && args.use_bulk;
     for (int i = tid; i < SG_EXP_TAB_LEN; i += NT)
@@ -268,31 +269,60 @@ __global__ void __launch_bounds__(NW * 32, MINB) sg_decode_kernel(const __grid_c
                     S.ngmax = 0;
                 }
                 __syncthreads();
-                for (;;) {
-                    int l = 0;
-                    if (lane == 0)
-                        l = atomicAdd(&S.line_next, 1);
-                    l = __shfl_sync(SG_FULL, l, 0);
-                    if (l >= 256)
-                        break;
-                    const int pos = sg_pos(axis, l, lane & 15);
-                    double v = 1.0;
-                    if (lane < 16) { /* L_ch + (alpha*L_E) */
-                        v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, S.le[pos]));
+                if constexpr (LPW == 2) {
+                    /* the warp takes two lines at a time, one per half, and
+                     * decodes them in lockstep (sg_line16.cuh) */
+                    const int hb = lane & 16, sl = lane & 15;
+                    SgWarpScratch* wsl = &S.ws[2 * warp + (hb >> 4)];
+                    for (;;) {
+                        int l = 0;
+                        if (lane == 0)
+                            l = atomicAdd(&S.line_next, 2);
+                        l = __shfl_sync(SG_FULL, l, 0) + (hb >> 4);
+                        if (l >= 256) /* 256 lines: both halves leave together */
+                            break;
+                        const int pos = sg_pos(axis, l, sl);
+                        const double le0 = S.le[pos];
+                        const double v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, le0));
                         if (args.ckpt)
-                            args.ckpt[(cw * (3ull * args.imax) + 3 * (iter - 1) + axis) * SG_CUBE + pos] = S.le[pos];
-                    }
-                    const SgLineResult r =
-                        sg_decode_line<G, false, CR>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
-                    if (lane < 16) {
+                            args.ckpt[(cw * (3ull * args.imax) + 3 * (iter - 1) + axis) * SG_CUBE + pos] = le0;
+                        const SgLineResult r = sg_decode_line16<G, CR>(v, lp, args.enum_tabs, S.etab, S.ltab, wsl);
                         S.le[pos] = r.le;
                         if (args.lapp)
                             args.lapp[cw * SG_CUBE + pos] = r.lapp;
+                        if (sl == 0) {
+                            S.hdw[l] = (uint16_t)r.hdword;
+                            atomicAdd(&S.ng, (unsigned long long)r.T);
+                            atomicMax(&S.ngmax, r.T);
+                        }
                     }
-                    if (lane == 0) {
-                        S.hdw[l] = (uint16_t)r.hdword;
-                        atomicAdd(&S.ng, (unsigned long long)r.T);
-                        atomicMax(&S.ngmax, r.T);
+                } else {
+                    for (;;) {
+                        int l = 0;
+                        if (lane == 0)
+                            l = atomicAdd(&S.line_next, 1);
+                        l = __shfl_sync(SG_FULL, l, 0);
+                        if (l >= 256)
+                            break;
+                        const int pos = sg_pos(axis, l, lane & 15);
+                        double v = 1.0;
+                        if (lane < 16) { /* L_ch + (alpha*L_E) */
+                            v = __dadd_rn(LCH_SMEM ? S.lch[pos] : __ldg(g + pos), __dmul_rn(alpha, S.le[pos]));
+                            if (args.ckpt)
+                                args.ckpt[(cw * (3ull * args.imax) + 3 * (iter - 1) + axis) * SG_CUBE + pos] = S.le[pos];
+                        }
+                        const SgLineResult r =
+                            sg_decode_line<G, false, CR>(v, lp, args.enum_tabs, S.etab, S.ltab, &S.ws[warp]);
+                        if (lane < 16) {
+                            S.le[pos] = r.le;
+                            if (args.lapp)
+                                args.lapp[cw * SG_CUBE + pos] = r.lapp;
+                        }
+                        if (lane == 0) {
+                            S.hdw[l] = (uint16_t)r.hdword;
+                            atomicAdd(&S.ng, (unsigned long long)r.T);
+                            atomicMax(&S.ngmax, r.T);
+                        }
                     }
                 }
                 __syncthreads();
@@ -501,7 +531,9 @@ __global__ void __launch_bounds__(256) sg_summary_kernel(const sg_cw_stats* __re
 
 /* Decoder kernel configurations: warps per codeword CTA, channel cube in
  * shared memory (bulk copy) or read from global memory, minimum resident
- * CTAs per SM for the register budget. */
+ * CTAs per SM for the register budget, error patterns per lane per step,
+ * and lines per warp (1: 32 lanes per line, sg_line.cuh; 2: 16 lanes per
+ * line, sg_line16.cuh). */
 struct SgVariant {
     const char* name;
     int nw;
@@ -514,6 +546,9 @@ struct SgVariant {
 #define SG_VARIANT(NW, L, M, G, NAME)                                                               \
     { NAME, NW, L, sizeof(SgCwSmem<NW, L>), (const void*)sg_decode_kernel<NW, L, M, G, false>, \
       (const void*)sg_decode_kernel<NW, L, M, G, true> }
+#define SG_VARIANT_L2(NW, M, G, NAME)                                                                          \
+    { NAME, NW, false, sizeof(SgCwSmem<NW, false, 2>), (const void*)sg_decode_kernel<NW, false, M, G, false, 2>, \
+      (const void*)sg_decode_kernel<NW, false, M, G, true, 2> }
 static const SgVariant g_variants[] = {
     SG_VARIANT(8, false, 3, 1, "w8-gmem"),
     SG_VARIANT(8, true, 2, 1, "w8-smem"),
@@ -522,6 +557,10 @@ static const SgVariant g_variants[] = {
     SG_VARIANT(16, false, 2, 2, "w16-gmem-g2"),
     SG_VARIANT(8, false, 3, 2, "w8-gmem-g2"),
     SG_VARIANT(12, true, 2, 2, "w12-smem-g2"),
+    SG_VARIANT_L2(8, 2, 2, "w8-l2-g2"),
+    SG_VARIANT_L2(8, 2, 4, "w8-l2-g4"),
+    SG_VARIANT_L2(10, 2, 2, "w10-l2-g2"),
+    SG_VARIANT_L2(16, 1, 2, "w16-l2-g2"),
 };
 #define SG_NVARIANTS ((int)(sizeof(g_variants) / sizeof(g_variants[0])))
 
@@ -561,7 +600,8 @@ static_assert(sg_tables_aligned<SgPersistSmem<24, 3>>() && sg_tables_aligned<SgP
                   sg_tables_aligned<SgPersistSmem<16, 3>>() && sg_tables_aligned<SgPersistSmem<20, 4>>() && sg_tables_aligned<SgPersistSmem<32, 3>>() &&
                   sg_tables_aligned<SgCwSmem<8, false>>() && sg_tables_aligned<SgCwSmem<8, true>>() &&
                   sg_tables_aligned<SgCwSmem<12, true>>() && sg_tables_aligned<SgCwSmem<16, false>>() &&
-                  sg_tables_aligned<SgLineSmem>(),
+                  sg_tables_aligned<SgCwSmem<8, false, 2>>() && sg_tables_aligned<SgCwSmem<10, false, 2>>() &&
+                  sg_tables_aligned<SgCwSmem<16, false, 2>>() && sg_tables_aligned<SgLineSmem>(),
               "shared table alignment");
 template <class T>
 constexpr bool sg_bulk_aligned()
@@ -573,8 +613,14 @@ static_assert(sg_bulk_aligned<SgCwSmem<8, true>>() && sg_bulk_aligned<SgCwSmem<1
 static_assert(sizeof(SgPersistSmem<32, 3>) <= 227 * 1024 && sizeof(SgPersistSmem<28, 3>) <= 227 * 1024 &&
                   sizeof(SgPersistSmem<24, 3>) <= 227 * 1024 && sizeof(SgPersistSmem<20, 4>) <= 227 * 1024 &&
                   sizeof(SgPersistSmem<16, 3>) <= 227 * 1024 && sizeof(SgCwSmem<8, true>) <= 227 * 1024 &&
-                  sizeof(SgCwSmem<16, false>) <= 227 * 1024 && sizeof(SgCwSmem<12, true>) <= 227 * 1024,
+                  sizeof(SgCwSmem<16, false>) <= 227 * 1024 && sizeof(SgCwSmem<12, true>) <= 227 * 1024 &&
+                  sizeof(SgCwSmem<16, false, 2>) <= 227 * 1024,
               "shared memory per CTA");
+/* the two-lines-per-warp configurations built for two CTAs per SM fit them
+ * (228 KB per SM, 1 KB of it reserved per CTA) */
+static_assert(2 * (sizeof(SgCwSmem<8, false, 2>) + 1024) <= 228 * 1024 &&
+                  2 * (sizeof(SgCwSmem<10, false, 2>) + 1024) <= 228 * 1024,
+              "two CTAs per SM");
 
 /* Static device memory of the allocation-free entry point: the error flag
  * (first 256 bytes), then per-codeword statistics and bits for at most
