@@ -725,7 +725,7 @@ sg_status host_init_locked()
     sg_code_build(&g_code);
     g_enum_host.assign((size_t)SG_ENUM_NTAB * SG_ENUM_LEN, 0);
     for (int ic = 0; ic < SG_ENUM_NTAB; ic++)
-        if (sg_enum_build(ic, g_enum_host.data() + (size_t)ic * SG_ENUM_LEN) != SG_ENUM_LEN)
+        if (sg_enum_build_impl(ic, g_enum_host.data() + (size_t)ic * SG_ENUM_LEN) != SG_ENUM_LEN)
             return fail(SG_ERR_ARG, "error-pattern order table incomplete");
     g_host_ready = true;
     return SG_OK;
@@ -1062,7 +1062,7 @@ size_t sg_pattern_order(int32_t ic, uint32_t* out, size_t cap)
     if (ic < 0 || !out)
         return 0;
     std::vector<uint32_t> t(SG_ENUM_LEN);
-    const size_t n = sg_enum_build(ic, t.data());
+    const size_t n = sg_enum_build_impl(ic, t.data());
     const size_t m = n < cap ? n : cap;
     for (size_t i = 0; i < m; i++)
         out[i] = sg_ent_pattern(t[i]) | (t[i] & SG_ENUM_GS);

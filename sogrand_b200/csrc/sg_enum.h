@@ -60,17 +60,6 @@ SG_HD uint32_t sg_ent_pattern(uint32_t ent)
 #define SG_ENUM_IC_CANON 56
 #define SG_ENUM_NTAB (SG_ENUM_IC_CANON + 1)
 
-#ifdef __cplusplus
-extern "C" {
-#endif
-/* Writes the pattern order for `ic` (ic >= 0) to out[0..SG_ENUM_LEN) and
- * returns the number of patterns written: SG_ENUM_LEN on success, 0 if the
- * successor logic left its domain (never for 0 <= ic < 2^20). */
-size_t sg_enum_build(int32_t ic, uint32_t* out);
-#ifdef __cplusplus
-}
-#endif
-
 /* mountain_build (cubic_decoder_final.c:775-789): set u[k+1..w) to u[k],
  * then pile the weight still missing onto the high end, n1 at a time. */
 SG_HD bool sg_enum_fill(int32_t* u, int32_t k, int32_t w, int32_t W1, int32_t n1)
@@ -115,7 +104,10 @@ SG_HD uint32_t sg_enum_entry(uint32_t m, uint32_t flag)
     return sg_swz(m & 0xffu) | (m & 0xff00u) | flag | (o1 << 17) | (o2 << 24) | (hi ? SG_ENUM_HI3 : 0u);
 }
 
-/* The builder itself, usable on host and device (same source, same order). */
+/* The builder, usable on host and device (same source, same order): writes
+ * the pattern order for `ic` (ic >= 0) to out[0..SG_ENUM_LEN) and returns the
+ * number of patterns written: SG_ENUM_LEN on success, 0 if the successor
+ * logic left its domain (never for 0 <= ic < 2^20). */
 SG_HD size_t sg_enum_build_impl(int32_t ic, uint32_t* out)
 {
     const int32_t n = 16;

@@ -1,4 +1,4 @@
-"""Error-pattern order tables (sg_enum.cpp) against the oracle's own
+"""Error-pattern order tables (sg_enum.h, built by the library) against the oracle's own
 restatement of the reference loops."""
 import ctypes as C
 
