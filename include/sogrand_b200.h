@@ -228,7 +228,9 @@ sg_status sg_encode_host(const uint8_t* info, size_t n_cw, uint8_t* code_bits);
 /* Full synthetic channel output for codewords [cw0, cw0+n_cw): info bits
  * (nullable) and float64 LLR cubes.  sigma > 0 fixes the noise deviation;
  * sigma <= 0 draws each codeword's Eb/N0 uniformly from
- * [ebn0_lo_db, ebn0_hi_db] with the decoder's own exp. */
+ * [ebn0_lo_db, ebn0_hi_db] with the decoder's own exp.  The device form
+ * writes the same values on the device (asynchronously on `stream`); its
+ * llr must be 8-byte aligned (16-byte aligned output is stored faster). */
 sg_status sg_gen_llr_host(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma,
                           double ebn0_lo_db, double ebn0_hi_db, uint8_t* info, double* llr);
 sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sigma,

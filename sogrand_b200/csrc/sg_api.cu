@@ -433,6 +433,7 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
     __shared__ alignas(16) double etab[SG_EXP_TAB_LEN];
     __shared__ alignas(16) double ltab[SG_LOG_TAB_LEN];
     __shared__ uint16_t W[256];
+    __shared__ alignas(16) double stage[SG_CUBE]; /* the codeword's LLRs, stored coalesced */
     __shared__ uint8_t ib[SG_INFO_BYTES];
     __shared__ uint8_t prow[8];
     __shared__ uint8_t ptab[256];
@@ -453,15 +454,80 @@ __global__ void __launch_bounds__(SG_THREADS) sg_gen_kernel(uint64_t seed, uint6
                 ib[tid * 8 + q] = (uint8_t)(r >> (8 * q));
         }
         __syncthreads();
-        if (tid == 0)
-            sg_encode_words(ib, prow, ptab, W);
+        /* sg_encode_words, each of its four stages spread over the block:
+         * info words, parity columns of the first 8 slices, parity rows,
+         * parity slices (the same words, every one written once) */
+        if (tid < 64)
+            W[(tid >> 3) * 16 + (tid & 7)] = (uint16_t)sg_brev8(ib[tid]);
+        __syncthreads();
+        if (tid < 64) {
+            const int l = tid >> 3, jj = tid & 7;
+            uint16_t acc = 0;
+            for (int j = 0; j < 8; j++)
+                if ((prow[j] >> jj) & 1)
+                    acc ^= W[l * 16 + j];
+            W[l * 16 + 8 + jj] = acc;
+        }
+        __syncthreads();
+        if (tid < 128) {
+            const uint16_t x = W[tid];
+            W[tid] = (uint16_t)((x & 0xff) | (ptab[x & 0xff] << 8));
+        }
+        __syncthreads();
+        if (tid < 128) {
+            const int jj = tid >> 4, j = tid & 15;
+            uint16_t acc = 0;
+            for (int l = 0; l < 8; l++)
+                if ((prow[l] >> jj) & 1)
+                    acc ^= W[l * 16 + j];
+            W[(8 + jj) * 16 + j] = acc;
+        }
         if (info && tid < SG_INFO_BYTES)
             info[c * SG_INFO_BYTES + tid] = ib[tid];
         __syncthreads();
         const double s = sigma > 0.0 ? sigma : sg_sigma_draw(seed, gc, lo, hi, etab);
-        for (int p = tid; p < SG_CUBE; p += SG_THREADS) {
-            const int bit = (W[p >> 4] >> (p & 15)) & 1;
-            llr[c * SG_CUBE + p] = sg_llr_of(bit, s, sg_normal(seed, gc, (uint32_t)p, ltab));
+        /* sg_normal for this thread's 16 positions p = tid + 256k, taken as
+         * one stream of polar attempts: every pass makes one attempt for every
+         * lane and a lane moves to its next position when its pair is
+         * accepted, so a warp no longer waits, position by position, for its
+         * unluckiest lane.  Each position keeps its first accepted attempt
+         * (after SG_POLAR_TRIES rejections, 0), as sg_normal does; the LLRs
+         * are staged in shared memory and stored coalesced. */
+        int k = 0;
+        uint64_t att = 0;
+        while (k < SG_CUBE / SG_THREADS) {
+            const uint32_t p = (uint32_t)(tid + SG_THREADS * k);
+            const uint64_t ctr = gc * 4096u + p;
+            const double u = sg_sym_unit(sg_rand(seed, 1 + 2 * att, ctr));
+            const double v = sg_sym_unit(sg_rand(seed, 2 + 2 * att, ctr));
+            const double uu = u * u;
+            const double vv = v * v;
+            const double ss = uu + vv;
+            const bool ok = ss > 0.0 && ss < 1.0;
+            if (ok || att + 1 == SG_POLAR_TRIES) {
+                double z = 0.0;
+                if (ok) {
+                    const double l = sg_log(ss, ltab);
+                    const double m = -2.0 * l;
+                    const double q = m / ss;
+                    z = u * __dsqrt_rn(q);
+                }
+                const int bit = (W[p >> 4] >> (p & 15)) & 1;
+                stage[p] = sg_llr_of(bit, s, z);
+                k++;
+                att = 0;
+            } else {
+                att++;
+            }
+        }
+        __syncthreads();
+        double* out = llr + c * SG_CUBE;
+        if (((uintptr_t)llr & 15u) == 0) {
+            for (int q = tid; q < SG_CUBE / 2; q += SG_THREADS)
+                reinterpret_cast<double2*>(out)[q] = reinterpret_cast<const double2*>(stage)[q];
+        } else {
+            for (int q = tid; q < SG_CUBE; q += SG_THREADS)
+                out[q] = stage[q];
         }
         __syncthreads();
     }
@@ -1047,6 +1113,8 @@ sg_status sg_gen_llr_device(uint64_t seed, uint64_t cw0, size_t n_cw, double sig
         return SG_OK;
     if (!d_llr)
         return fail(SG_ERR_ARG, "llr is NULL");
+    if ((uintptr_t)d_llr & 7u)
+        return fail(SG_ERR_ARG, "llr must be 8-byte aligned");
     DevCtx* c = nullptr;
     sg_status s = get_ctx(&c);
     if (s != SG_OK)

@@ -47,25 +47,33 @@ SG_HD double sg_sym_unit(uint64_t r)
 SG_HD double sg_normal(uint64_t seed, uint64_t c, uint32_t p, const double* ltab)
 {
     uint64_t ctr = c * 4096u + p;
+    /* draw until a pair lands inside the unit disc; the transform runs once,
+     * after the loop, so that lanes needing different numbers of draws
+     * share it on a GPU */
+    double u = 0.0, s = 0.0;
+    int ok = 0;
     for (uint64_t a = 0; a < SG_POLAR_TRIES; a++) {
-        double u = sg_sym_unit(sg_rand(seed, 1 + 2 * a, ctr));
+        u = sg_sym_unit(sg_rand(seed, 1 + 2 * a, ctr));
         double v = sg_sym_unit(sg_rand(seed, 2 + 2 * a, ctr));
         double uu = u * u;
         double vv = v * v;
-        double s = uu + vv;
+        s = uu + vv;
         if (s > 0.0 && s < 1.0) {
-            double l = sg_log(s, ltab);
-            double m = -2.0 * l;
-            double q = m / s;
-#if defined(__CUDA_ARCH__)
-            double f = __dsqrt_rn(q);
-#else
-            double f = sqrt(q);
-#endif
-            return u * f;
+            ok = 1;
+            break;
         }
     }
-    return 0.0;
+    if (!ok)
+        return 0.0;
+    double l = sg_log(s, ltab);
+    double m = -2.0 * l;
+    double q = m / s;
+#if defined(__CUDA_ARCH__)
+    double f = __dsqrt_rn(q);
+#else
+    double f = sqrt(q);
+#endif
+    return u * f;
 }
 
 /* Noise deviation of codeword c when Eb/N0 is drawn uniformly from

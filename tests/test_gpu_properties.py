@@ -40,6 +40,29 @@ def test_device_generator_equals_host(cuda, sg):
         assert np.array_equal(dl.cpu().numpy().view(np.int64), hl.view(np.int64))
 
 
+def test_device_generator_unaligned_output(cuda, sg):
+    """LLR output that is 8- but not 16-byte aligned takes the generator's
+    scalar stores and gives the same values; output that is not 8-byte
+    aligned is rejected."""
+    from sogrand_b200 import _lib
+
+    torch = cuda
+    lib = _lib.load()
+    n = 5
+    hi, hl = sg.gen_llr(321, 7, n, ebn0_range=(1.0, 3.0))
+    buf = torch.zeros(n * 4096 + 2, dtype=torch.float64, device="cuda")
+    base = buf.data_ptr()
+    assert base % 16 == 0
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.sg_gen_llr_device(321, 7, n, 0.0, 1.0, 3.0, None, base + 8, stream) == 0
+    torch.cuda.synchronize()
+    got = buf[1:1 + n * 4096].cpu().numpy().reshape(n, 4096)
+    assert np.array_equal(got.view(np.int64), hl.view(np.int64))
+    assert buf[0].item() == 0.0 and buf[-1].item() == 0.0
+    assert lib.sg_gen_llr_device(321, 7, n, 0.0, 1.0, 3.0, None, base + 4, stream) == 1
+    assert b"8-byte aligned" in lib.sg_last_error()
+
+
 def test_device_api_equals_host_api_and_batching(cuda, sg):
     torch = cuda
     _, llr = sg.gen_llr(7, 0, 24, ebn0_db=1.5)
