@@ -117,26 +117,35 @@ def test_early_termination_oracle(libm, sg):
 
 
 def test_large_fixture_pinned_by_restatements(sg, oracle_paths):
-    """golden_large.npz (4096 codewords at 2.0 and 1.5 dB, decoded by the
-    reference, by the reference under a correctly rounded libm, and by the
-    table-math restatement): its inputs regenerate, and on sampled codewords
-    -- every recorded mismatch with the glibc-linked reference among them --
-    the table-math oracle reproduces the twin entries and the correctly
-    rounded oracle the ref_cr entries."""
+    """golden_large.npz (large sets decoded by the reference, by the
+    reference under a correctly rounded libm, and by the table-math
+    restatement): its inputs regenerate, and on sampled codewords -- every
+    recorded mismatch with the glibc-linked reference among them, and under
+    a Tmax cap some whose reference output is undefined -- the table-math
+    oracle reproduces the twin entries and the correctly rounded oracle the
+    ref_cr entries (where the reference defines them)."""
     import os
 
     z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_large.npz"))
+    names = sorted({k.split("/")[0] for k in z.files if k.endswith("/meta")})
     jobs, want = [], []
-    for name in ("large_2.0dB", "large_1.5dB"):
+    for name in names:
         seed, n = (int(v) for v in z[f"{name}/meta"])
+        tmax = int(z[f"{name}/tmax"]) if f"{name}/tmax" in z.files else UINT64_MAX
         _, llr = sg.gen_llr(seed, 0, n, ebn0_db=float(z[f"{name}/ebn0_db"]))
         assert hashlib.sha256(llr.tobytes()).hexdigest() == str(z[f"{name}/llr_sha256"]), name
+        undef = (z[f"{name}/ref_cr_undefined"].astype(bool) if f"{name}/ref_cr_undefined" in z.files
+                 else np.zeros(n, bool))
         for kind, lib in (("twin", "twin"), ("ref_cr", "twin_cr")):
             bits = z[f"{name}/ref_bits"].copy()
             bits[z[f"{name}/{kind}_bits_diff_idx"]] = z[f"{name}/{kind}_bits_diff"]
-            idx = sorted(set(z[f"{name}/ref_vs_{kind}_idx"].tolist()) | {0, n - 1})
-            for i in idx:
-                jobs.append((oracle_paths[lib], llr[i], {}))
+            idx = set(z[f"{name}/ref_vs_{kind}_idx"].tolist()) | {0, n - 1}
+            if kind == "twin":
+                idx |= set(np.flatnonzero(undef)[:4].tolist())
+            else:
+                idx = {i for i in idx if not undef[i]}
+            for i in sorted(idx):
+                jobs.append((oracle_paths[lib], llr[i], {"Tmax": tmax}))
                 want.append((name, kind, i, bits[i].tobytes(),
                              tuple(int(z[f"{name}/{kind}_{f}"][i]) for f in ("ng", "ng_p", "converged")),
                              float(z[f"{name}/{kind}_iterations"][i])))
