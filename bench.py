@@ -520,9 +520,18 @@ def main():
                "d2h_bytes_per_step": n * (64 + sg.STATS_DTYPE.itemsize),
                "api": "sg_decode_host (host buffers, copies inside the timed region)"}
 
-    ceil, ceil_other = C.c_double(), C.c_double()
-    _lib.check(lib.sg_guess_ceiling(20000, args.math, C.byref(ceil)))
-    _lib.check(lib.sg_guess_ceiling(20000, 1 - args.math, C.byref(ceil_other)))
+    def best_ceiling(mode, runs=3):
+        """The per-guess ceiling is the best rate the GPU reaches: the
+        maximum of a few ~20 ms measurements (single ones vary by up to 8 %
+        between runs)."""
+        v = C.c_double()
+        best = 0.0
+        for _ in range(runs):
+            _lib.check(lib.sg_guess_ceiling(20000, mode, C.byref(v)))
+            best = max(best, v.value)
+        return C.c_double(best)
+
+    ceil, ceil_other = best_ceiling(args.math), best_ceiling(1 - args.math)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -546,7 +555,7 @@ def main():
                               "peak": ceil.value, "unit": "guess/s per GPU",
                               "frac": value * ng_per_cw / world / ceil.value,
                               "how": "sg_guess_ceiling: PM add + exp(-PM) + P_notGuess subtract per guess, "
-                                     "all SMs, measured on this GPU in this run, with the exp of the math "
+                                     "all SMs, measured on this GPU in this run (best of 3), with the exp of the math "
                                      "mode used (" + ("table-driven" if args.math == 0 else "correctly rounded")
                                      + ")",
                               "peak_other_math_mode": ceil_other.value},
