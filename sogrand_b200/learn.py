@@ -6,7 +6,11 @@ decoder.
 
 Training: Adam on 3*Imax weights (initialised to the reference's 0.7) with
 the BCE of the final APP, or of every phase's APP (--loss phases), on fresh
-seeded codewords (sogrand_b200.diff).
+seeded codewords (sogrand_b200.diff).  Or, with --search, no gradient: every
+linear weight ramp alpha_p = a + b*p/(3*Imax-1) of a grid decodes the same
+search batch and the ramp with the lowest BER is kept (the BCE gradient
+holds the decode's discrete branch fixed, while the weights move BER mostly
+through that branch).
 Evaluation: the plain decoder (alpha = 0.7, Imax = 30, and at each evaluated
 Imax) and the learned weights at each Imax decode the same fresh codewords
 (a codeword range of the seeded stream disjoint from training).  Every
@@ -98,6 +102,56 @@ def evaluate_set(configs: dict, ebn0: float, n_cw: int, seed: int, cw0: int, chu
     return out
 
 
+def schedule(a: float, b: float, imax: int) -> np.ndarray:
+    """Per-phase weights alpha_p = a + b * p / (3*Imax - 1), p = 0 .. 3*Imax-1
+    (a linear ramp over the decode; b = 0 is a constant, and a = 0.7, b = 0
+    the reference's weights), clipped to [0.05, 1.5]."""
+    n = 3 * imax
+    t = np.arange(n) / max(n - 1, 1)
+    return np.clip(a + b * t, 0.05, 1.5)
+
+
+def search_schedules(imax: int, ebn0: float, n_cw: int, seed: int, a_grid, b_grid, chunk: int = 100000) -> dict:
+    """Derivative-free search for weights: every ramp (a, b) of the grid and
+    the reference's weights decode the same n_cw codewords at Imax; each
+    ramp is scored by its paired BER difference from the reference's.
+    Returns the table and the best ramp (lowest BER)."""
+    configs = {"plain": (None, imax)}
+    names = {}
+    for a in a_grid:
+        for b in b_grid:
+            k = f"a{a:.2f}_b{b:+.2f}"
+            names[k] = (float(a), float(b))
+            configs[k] = (schedule(a, b, imax), imax)
+    row = evaluate_set(configs, ebn0, n_cw, seed, 0, chunk=chunk, pairs=[(k, "plain") for k in names])
+    table = []
+    for pr in row["paired"]:
+        a, b = names[pr["a"]]
+        c = row["configs"][pr["a"]]
+        table.append({"a": a, "b": b, "ber": c["ber"], "ber_diff_vs_plain": pr["ber_diff"], "ci95": pr["ci95"],
+                      "avg_iterations": c["avg_iterations"]})
+    best = min(table, key=lambda r: r["ber"])
+    return {"imax": imax, "ebn0_db": ebn0, "codewords": n_cw, "seed": seed,
+            "plain_ber": row["configs"]["plain"]["ber"], "table": table, "best": best}
+
+
+def search_schedules_multi(imax: int, points, seed: int, a_grid, b_grid) -> dict:
+    """search_schedules at several (Eb/N0, codewords) points; the kept ramp
+    is the one whose worst relative BER change from the reference's weights
+    over the points is lowest (below 0: better at every point)."""
+    runs = [search_schedules(imax, eb, n, seed + 1000 * i, a_grid, b_grid) for i, (eb, n) in enumerate(points)]
+    score = {}
+    for run in runs:
+        for r in run["table"]:
+            rel = r["ber"] / run["plain_ber"] - 1.0 if run["plain_ber"] else 0.0
+            key = (r["a"], r["b"])
+            score[key] = max(score.get(key, -math.inf), rel)
+    (a, b), worst = min(score.items(), key=lambda kv: kv[1])
+    return {"imax": imax, "points": [{"ebn0_db": eb, "codewords": n} for eb, n in points], "runs": runs,
+            "worst_relative_ber_change": [{"a": k[0], "b": k[1], "worst": v} for k, v in score.items()],
+            "best": {"a": a, "b": b, "worst_relative_ber_change": worst}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=60)
@@ -114,6 +168,14 @@ def main():
     ap.add_argument("--eval-imax", default="5,10,30")
     ap.add_argument("--no-plain-same-imax", action="store_true",
                     help="compare only against the plain decoder at Imax 30")
+    ap.add_argument("--search", action="store_true",
+                    help="instead of gradient training, pick the best linear weight ramp by BER (search_schedules)")
+    ap.add_argument("--search-cw", default="200000",
+                    help="search codewords, one number or one per --search-ebn0 point")
+    ap.add_argument("--search-ebn0", default=None,
+                    help="search points (dB, comma list; default --train-ebn0); several: minimax over them")
+    ap.add_argument("--search-a", default="0.5,0.6,0.7,0.8,0.9,1.0")
+    ap.add_argument("--search-b", default="-0.4,-0.2,0,0.2,0.4")
     ap.add_argument("--seed", type=int, default=90210)
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
@@ -121,8 +183,27 @@ def main():
     from sogrand_b200 import diff
 
     t0 = time.perf_counter()
+    search = None
     if args.weights:
         alpha = np.array(json.load(open(args.weights))["weights"])
+        hist = []
+    elif args.search:
+        agrid = [float(x) for x in args.search_a.split(",")]
+        bgrid = [float(x) for x in args.search_b.split(",")]
+        ebs = [float(x) for x in args.search_ebn0.split(",")] if args.search_ebn0 else [args.train_ebn0]
+        cws = [int(x) for x in args.search_cw.split(",")]
+        cws = cws * len(ebs) if len(cws) == 1 else cws
+        if len(ebs) == 1:
+            search = search_schedules(args.imax_train, ebs[0], cws[0], args.seed, agrid, bgrid)
+            tables = [search]
+        else:
+            search = search_schedules_multi(args.imax_train, list(zip(ebs, cws)), args.seed, agrid, bgrid)
+            tables = search["runs"]
+        for run in tables:
+            for r in run["table"]:
+                print(f"{run['ebn0_db']} dB a {r['a']:.2f} b {r['b']:+.2f} BER {r['ber']:.4e} vs plain "
+                      f"{r['ber_diff_vs_plain']:+.3e} [{r['ci95'][0]:+.2e}, {r['ci95'][1]:+.2e}]", flush=True)
+        alpha = schedule(search["best"]["a"], search["best"]["b"], args.imax_train)
         hist = []
     else:
         alpha, hist = diff.train_weights(steps=args.steps, batch=args.batch, ebn0_db=args.train_ebn0,
@@ -134,7 +215,7 @@ def main():
            "train": {"steps": args.steps, "batch": args.batch, "val_cw": args.val_cw, "loss": args.loss,
                      "ebn0_db": args.train_ebn0, "imax": args.imax_train, "lr": args.lr, "history": hist,
                      "seconds": train_s},
-           "eval": []}
+           "search": search, "eval": []}
     eval_seed = args.seed + 1  # a stream disjoint from training
     imaxes = [int(x) for x in args.eval_imax.split(",")]
     configs = {"plain30": (None, 30)}
